@@ -1,0 +1,339 @@
+"""basements_b200 — B200-native MLS-MPM soil step behind the bm_* C ABI.
+
+Python access to ``libbm_mpm.so`` through ctypes, mirroring the reference
+``basements::mpm::MPMSolver`` API (include/basements/physics/mpm/mpm_solver.h:15-95)
+and the coupler plug-in ``MPMRigidCouplerPIC::apply``
+(include/basements/physics/coupling/mpm_rigid_coupler_pic.h:88-184). The
+computation always runs in the CUDA library; if the library is missing this
+module raises at import of ``lib()``; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbm_mpm.so")
+
+BM_OK = 0
+STATUS_NAMES = {
+    0: "BM_OK", 1: "BM_ERR_INVALID_ARGUMENT", 2: "BM_ERR_OUT_OF_MEMORY", 3: "BM_ERR_CUDA",
+    4: "BM_ERR_DOMAIN_ESCAPE", 5: "BM_ERR_NON_FINITE", 6: "BM_ERR_TIMEOUT", 7: "BM_ERR_NOT_FOUND",
+    8: "BM_ERR_STATE", 9: "BM_ERR_NO_DEVICE",
+}
+
+
+class BMError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)} {detail}".strip())
+
+
+class Domain(C.Structure):
+    _fields_ = [("origin", C.c_int32 * 3), ("extent", C.c_int32 * 3)]
+
+
+class Collider(C.Structure):
+    """bm_collider_t: the fields of RigidColliderState (mpm_rigid_coupler.h:72-84)."""
+    _fields_ = [
+        ("center", C.c_float * 3),
+        ("orientation", C.c_float * 4),
+        ("half_extents", C.c_float * 3),
+        ("linear_velocity", C.c_float * 3),
+        ("angular_velocity", C.c_float * 3),
+        ("friction", C.c_float),
+        ("mass", C.c_float),
+        ("shape", C.c_int32),
+    ]
+
+
+class Reaction(C.Structure):
+    _fields_ = [("force", C.c_float * 3), ("torque", C.c_float * 3), ("nodes_inside", C.c_int32)]
+
+
+class ParticlesView(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_float)) for n in ("position", "velocity", "F", "C", "mass", "volume")]
+
+
+_f = C.POINTER(C.c_float)
+_i32 = C.POINTER(C.c_int32)
+_u8 = C.POINTER(C.c_uint8)
+_h = C.c_void_p
+_st = C.c_int
+
+_SIGS = {
+    "bm_get_version": (C.c_int, []),
+    "bm_status_string": (C.c_char_p, [C.c_int]),
+    "bm_last_error": (C.c_char_p, []),
+    "bm_set_device": (_st, [C.c_int32]),
+    "bm_solver_create": (_st, [C.c_float, C.POINTER(Domain), C.POINTER(_h)]),
+    "bm_solver_destroy": (_st, [_h]),
+    "bm_solver_set_domain": (_st, [_h, C.POINTER(Domain)]),
+    "bm_solver_get_domain": (_st, [_h, C.POINTER(Domain)]),
+    "bm_solver_set_auto_margin": (_st, [_h, C.c_int32]),
+    "bm_solver_set_material": (_st, [_h, C.c_float, C.c_float, C.c_float]),
+    "bm_solver_set_gravity": (_st, [_h, _f]),
+    "bm_solver_set_plastic_alpha": (_st, [_h, C.c_float]),
+    "bm_solver_set_floor_friction": (_st, [_h, C.c_float]),
+    "bm_solver_add_particles": (_st, [_h, C.c_int64, _f, _f, _f]),
+    "bm_solver_num_particles": (_st, [_h, C.POINTER(C.c_int64)]),
+    "bm_solver_get_particles": (_st, [_h, C.POINTER(ParticlesView)]),
+    "bm_solver_set_particles": (_st, [_h, C.c_int64, C.c_int64, C.POINTER(ParticlesView)]),
+    "bm_solver_step": (_st, [_h, C.c_float]),
+    "bm_solver_step_n": (_st, [_h, C.c_float, C.c_int32]),
+    "bm_solver_p2g": (_st, [_h, C.c_float]),
+    "bm_solver_grid_update": (_st, [_h, C.c_float]),
+    "bm_coupler_m1_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
+    "bm_solver_g2p": (_st, [_h, C.c_float]),
+    "bm_solver_step_coupled": (_st, [_h, C.c_float, C.c_int32, C.POINTER(Collider), C.POINTER(Reaction)]),
+    "bm_solver_get_reactions": (_st, [_h, C.c_int32, C.POINTER(Reaction)]),
+    "bm_solver_grid_num_nodes": (_st, [_h, C.POINTER(C.c_int64)]),
+    "bm_solver_get_grid": (_st, [_h, _f, _f, _f, _u8, _u8]),
+    "bm_solver_seed_grid": (_st, [_h, C.c_int64, _i32, _f, _f]),
+    "bm_solver_set_grid_velocity": (_st, [_h, _f]),
+    "bm_solver_sync": (_st, [_h, C.POINTER(C.c_int64)]),
+    "bm_solver_stream": (_st, [_h, C.POINTER(C.c_void_p)]),
+    "bm_solver_profile_enable": (_st, [_h, C.c_int32]),
+    "bm_solver_profile_read": (_st, [_h, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "bm_solver_profile_reset": (_st, [_h]),
+    "bm_solver_timer_start": (_st, [_h]),
+    "bm_solver_timer_stop": (_st, [_h, C.POINTER(C.c_double)]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m basements_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def set_device(device: int):
+    check(lib().bm_set_device(int(device)), "bm_set_device")
+
+
+def declared_symbols():
+    return list(_SIGS)
+
+
+def check(status: int, where: str):
+    if status != BM_OK:
+        detail = lib().bm_last_error().decode(errors="replace")
+        raise BMError(status, where, detail)
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(_f)
+
+
+def make_collider(center, half_extents, orientation=(1.0, 0.0, 0.0, 0.0), linear_velocity=(0, 0, 0),
+                  angular_velocity=(0, 0, 0), friction=0.5, mass=1.0, shape=0) -> Collider:
+    c = Collider()
+    c.center[:] = [float(v) for v in center]
+    c.orientation[:] = [float(v) for v in orientation]
+    c.half_extents[:] = [float(v) for v in half_extents]
+    c.linear_velocity[:] = [float(v) for v in linear_velocity]
+    c.angular_velocity[:] = [float(v) for v in angular_velocity]
+    c.friction = float(friction)
+    c.mass = float(mass)
+    c.shape = int(shape)
+    return c
+
+
+class MPMSolver:
+    """Device-resident MLS-MPM solver (one CUDA stream per instance)."""
+
+    def __init__(self, dx: float = 0.1, domain=None, margin: int | None = None):
+        L = lib()
+        self._h = C.c_void_p()
+        d = None
+        if domain is not None:
+            d = Domain()
+            d.origin[:] = [int(v) for v in domain[0]]
+            d.extent[:] = [int(v) for v in domain[1]]
+        check(L.bm_solver_create(float(dx), C.byref(d) if d is not None else None, C.byref(self._h)),
+              "bm_solver_create")
+        self.dx = float(dx)
+        if margin is not None:
+            check(L.bm_solver_set_auto_margin(self._h, int(margin)), "bm_solver_set_auto_margin")
+
+    # -- lifetime --------------------------------------------------------------
+    def close(self):
+        if self._h:
+            lib().bm_solver_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- MPMSolver API (mpm_solver.h:19-95) -----------------------------------
+    def set_material(self, young_modulus, poisson_ratio, bulk_density):
+        check(lib().bm_solver_set_material(self._h, young_modulus, poisson_ratio, bulk_density),
+              "bm_solver_set_material")
+
+    def set_gravity(self, g):
+        a = np.asarray(g, np.float32)
+        check(lib().bm_solver_set_gravity(self._h, _fp(a)), "bm_solver_set_gravity")
+
+    def set_plastic_alpha(self, a):
+        check(lib().bm_solver_set_plastic_alpha(self._h, a), "bm_solver_set_plastic_alpha")
+
+    def set_floor_friction(self, mu):
+        check(lib().bm_solver_set_floor_friction(self._h, mu), "bm_solver_set_floor_friction")
+
+    def add_particles(self, position, velocity=None, mass=None):
+        pos = np.ascontiguousarray(position, np.float32).reshape(-1, 3)
+        vel = None if velocity is None else np.ascontiguousarray(velocity, np.float32).reshape(-1, 3)
+        if mass is not None:
+            mass = np.ascontiguousarray(np.broadcast_to(np.asarray(mass, np.float32), (len(pos),)))
+        check(lib().bm_solver_add_particles(self._h, len(pos), _fp(pos), _fp(vel), _fp(mass)),
+              "bm_solver_add_particles")
+
+    def add_particle(self, position, velocity=(0.0, 0.0, 0.0), mass=1.0):
+        self.add_particles([position], [velocity], [mass])
+
+    def num_particles(self) -> int:
+        n = C.c_int64()
+        check(lib().bm_solver_num_particles(self._h, C.byref(n)), "bm_solver_num_particles")
+        return n.value
+
+    def get_particles(self, fields=("position", "velocity", "F", "C", "mass", "volume")):
+        n = self.num_particles()
+        shapes = {"position": (n, 3), "velocity": (n, 3), "F": (n, 3, 3), "C": (n, 3, 3), "mass": (n,),
+                  "volume": (n,)}
+        out = {k: np.empty(shapes[k], np.float32) for k in fields}
+        v = ParticlesView()
+        for k in out:
+            setattr(v, k, _fp(out[k]))
+        check(lib().bm_solver_get_particles(self._h, C.byref(v)), "bm_solver_get_particles")
+        return out
+
+    def set_particles(self, first=0, position=None, velocity=None, F=None, C_=None):
+        arrs = {"position": position, "velocity": velocity, "F": F, "C": C_}
+        arrs = {k: np.ascontiguousarray(a, np.float32) for k, a in arrs.items() if a is not None}
+        n = next(len(a) for a in arrs.values())
+        v = ParticlesView()
+        for k, a in arrs.items():
+            setattr(v, k, _fp(a))
+        check(lib().bm_solver_set_particles(self._h, int(first), int(n), C.byref(v)), "bm_solver_set_particles")
+
+    def step(self, dt, n_steps: int = 1):
+        if n_steps == 1:
+            check(lib().bm_solver_step(self._h, dt), "bm_solver_step")
+        else:
+            check(lib().bm_solver_step_n(self._h, dt, int(n_steps)), "bm_solver_step_n")
+
+    # -- split phases + coupler plug-in ----------------------------------------
+    def p2g(self, dt):
+        check(lib().bm_solver_p2g(self._h, dt), "bm_solver_p2g")
+
+    def grid_update(self, dt):
+        check(lib().bm_solver_grid_update(self._h, dt), "bm_solver_grid_update")
+
+    def g2p(self, dt):
+        check(lib().bm_solver_g2p(self._h, dt), "bm_solver_g2p")
+
+    def m1_apply(self, body: Collider, dt):
+        r = Reaction()
+        check(lib().bm_coupler_m1_apply(self._h, C.byref(body), dt, C.byref(r)), "bm_coupler_m1_apply")
+        return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
+
+    def step_coupled(self, dt, bodies, read_reactions=True):
+        n = len(bodies)
+        arr = (Collider * max(n, 1))(*bodies)
+        out = (Reaction * max(n, 1))() if read_reactions else None
+        check(lib().bm_solver_step_coupled(self._h, dt, n, arr, out if read_reactions else None),
+              "bm_solver_step_coupled")
+        if not read_reactions:
+            return None
+        return [(np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside))
+                for r in out[:n]]
+
+    # -- grid -------------------------------------------------------------------
+    def domain(self):
+        d = Domain()
+        check(lib().bm_solver_get_domain(self._h, C.byref(d)), "bm_solver_get_domain")
+        return tuple(d.origin), tuple(d.extent)
+
+    def get_grid(self):
+        """Dense grid over the box: dict of arrays shaped (ex, ey, ez, ...)."""
+        (o, e) = self.domain()
+        nn = e[0] * e[1] * e[2]
+        vel = np.empty((nn, 3), np.float32)
+        frc = np.empty((nn, 3), np.float32)
+        mass = np.empty(nn, np.float32)
+        act = np.empty(nn, np.uint8)
+        bal = np.empty(nn, np.uint8)
+        check(lib().bm_solver_get_grid(self._h, _fp(vel), _fp(frc), _fp(mass), act.ctypes.data_as(_u8),
+                                       bal.ctypes.data_as(_u8)), "bm_solver_get_grid")
+        sh = tuple(e)
+        return {"origin": np.array(o), "velocity": vel.reshape(*sh, 3), "force": frc.reshape(*sh, 3),
+                "mass": mass.reshape(sh), "active": act.reshape(sh), "block_allocated": bal.reshape(sh)}
+
+    def seed_grid(self, ijk, velocity, mass):
+        ijk = np.ascontiguousarray(ijk, np.int32).reshape(-1, 3)
+        vel = np.ascontiguousarray(velocity, np.float32).reshape(-1, 3)
+        m = np.ascontiguousarray(np.broadcast_to(np.asarray(mass, np.float32), (len(ijk),)))
+        check(lib().bm_solver_seed_grid(self._h, len(ijk), ijk.ctypes.data_as(_i32), _fp(vel), _fp(m)),
+              "bm_solver_seed_grid")
+
+    def set_grid_velocity(self, velocity):
+        v = np.ascontiguousarray(velocity, np.float32)
+        check(lib().bm_solver_set_grid_velocity(self._h, _fp(v)), "bm_solver_set_grid_velocity")
+
+    # -- status / profiling ----------------------------------------------------------
+    def sync(self):
+        """Waits for the stream; returns (status, escaped_writes) without raising."""
+        esc = C.c_int64()
+        st = lib().bm_solver_sync(self._h, C.byref(esc))
+        return st, esc.value
+
+    def profile(self, on=True):
+        check(lib().bm_solver_profile_enable(self._h, 1 if on else 0), "bm_solver_profile_enable")
+
+    def profile_reset(self):
+        check(lib().bm_solver_profile_reset(self._h), "bm_solver_profile_reset")
+
+    def timer_start(self):
+        check(lib().bm_solver_timer_start(self._h), "bm_solver_timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        check(lib().bm_solver_timer_stop(self._h, C.byref(ms)), "bm_solver_timer_stop")
+        return ms.value
+
+    def profile_read(self):
+        cap = 32
+        names = (C.c_char_p * cap)()
+        ms = (C.c_double * cap)()
+        cnt = (C.c_int64 * cap)()
+        n = C.c_int32()
+        check(lib().bm_solver_profile_read(self._h, cap, names, ms, cnt, C.byref(n)), "bm_solver_profile_read")
+        return {names[i].decode(): (ms[i], cnt[i]) for i in range(n.value)}

@@ -1,0 +1,172 @@
+"""Seeded synthetic scenes for the MLS-MPM soil step.
+
+No public dataset is involved; every workload is generated here from a seed.
+
+* ``sand_column``  — plain sand column collapse: 32^3 grid, dx = 1/32, cells
+  [8,24) x [2,10) x [8,24) at 8 particles per cell (16,384 particles), uniform
+  jitter drawn from MT19937(0) in the order x, y, z per particle with
+  (i, j, k, q) lexicographic, the way ``std::uniform_real_distribution<float>``
+  draws them; E = 3.5e5 Pa, nu = 0.3, rho = 1600, friction angle 30 deg,
+  dt = 1e-4.
+* ``wheel_rut``    — plain large rigid-wheel rut: 128^3 grid, dx = 1/128, sand
+  bed of 128 x 40 x 128 cells at 8 ppc (5,242,880 candidates) subsampled
+  without replacement to 2,000,000; M1 cylinder R = 0.1 m, width 0.08 m,
+  5 kg, rolling about z at -2 rad/s while translating at 0.1 m/s; dt = 5e-5.
+* ``scene_batch``  — uneven box-drop scenes for the batched form.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def dp_alpha(friction_angle_deg: float) -> float:
+    """alpha = sqrt(2/3) * 2 sin(phi) / (3 - sin(phi)) (mpm_solver.h:103)."""
+    s = math.sin(math.radians(friction_angle_deg))
+    return math.sqrt(2.0 / 3.0) * 2.0 * s / (3.0 - s)
+
+
+def mt19937_uniform_f32(seed: int, n: int) -> np.ndarray:
+    """n floats in [0, 1) as std::uniform_real_distribution<float>(0, 1) draws
+    them from std::mt19937(seed): one 32-bit word per float, word / 2^32
+    rounded to float, values that round to 1 moved to the largest float < 1."""
+    rs = np.random.RandomState(seed)
+    words = rs.randint(0, 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32)
+    u = words.astype(np.float32) / np.float32(2.0 ** 32)
+    u[u >= 1.0] = np.nextafter(np.float32(1.0), np.float32(0.0))
+    return u
+
+
+@dataclass
+class Body:
+    center: tuple
+    half_extents: tuple
+    orientation: tuple = (1.0, 0.0, 0.0, 0.0)
+    linear_velocity: tuple = (0.0, 0.0, 0.0)
+    angular_velocity: tuple = (0.0, 0.0, 0.0)
+    friction: float = 0.5
+    mass: float = 1.0
+    shape: int = 0
+    kinematic: bool = True
+
+    def at_time(self, t: float) -> "Body":
+        """Kinematic pose after time t (constant linear velocity; the angular
+        velocity is exchanged with the grid but the pose is not rotated)."""
+        c = tuple(float(self.center[a] + self.linear_velocity[a] * t) for a in range(3))
+        return Body(c, self.half_extents, self.orientation, self.linear_velocity, self.angular_velocity,
+                    self.friction, self.mass, self.shape, self.kinematic)
+
+    def as_tuple(self):
+        return dict(center=self.center, half_extents=self.half_extents, orientation=self.orientation,
+                    linear_velocity=self.linear_velocity, angular_velocity=self.angular_velocity,
+                    friction=self.friction, mass=self.mass, shape=self.shape)
+
+
+@dataclass
+class Scene:
+    name: str
+    dx: float
+    grid: int
+    position: np.ndarray
+    mass: np.ndarray
+    E: float
+    nu: float
+    rho: float
+    alpha: float
+    dt: float
+    steps: int
+    floor_friction: float = 0.4
+    gravity: tuple = (0.0, -9.81, 0.0)
+    bodies: list = field(default_factory=list)
+    domain: tuple | None = None  # ((ox, oy, oz), (ex, ey, ez)) in nodes
+
+    @property
+    def n(self) -> int:
+        return len(self.position)
+
+
+def sand_column(cells=(16, 8, 16), offset=(8, 2, 8), ppc=8, grid=32, seed=0) -> Scene:
+    dx = 1.0 / grid
+    ci, cj, ck = cells
+    n = ci * cj * ck * ppc
+    u = mt19937_uniform_f32(seed, 3 * n).reshape(ci, cj, ck, ppc, 3)
+    ii, jj, kk = np.meshgrid(np.arange(ci), np.arange(cj), np.arange(ck), indexing="ij")
+    cell = np.stack([ii + offset[0], jj + offset[1], kk + offset[2]], -1).astype(np.float32)
+    pos = ((cell[:, :, :, None, :] + u) * np.float32(dx)).astype(np.float32).reshape(-1, 3)
+    rho = 1600.0
+    m = np.float32(rho * dx ** 3 / ppc)
+    return Scene("sand_column", dx, grid, pos, np.full(n, m, np.float32), 3.5e5, 0.3, rho, dp_alpha(30.0),
+                 1e-4, 1000)
+
+
+def wheel_rut(n_keep=2_000_000, grid=128, bed_cells=(128, 40, 128), ppc=8, seed=1) -> Scene:
+    dx = 1.0 / grid
+    rng = np.random.default_rng(seed)
+    ncand = bed_cells[0] * bed_cells[1] * bed_cells[2] * ppc
+    keep = np.sort(rng.choice(ncand, size=min(n_keep, ncand), replace=False))
+    cell_id = keep // ppc
+    k = cell_id % bed_cells[2]
+    j = (cell_id // bed_cells[2]) % bed_cells[1]
+    i = cell_id // (bed_cells[2] * bed_cells[1])
+    jit = rng.random((len(keep), 3), dtype=np.float32)
+    pos = ((np.stack([i, j, k], -1).astype(np.float32) + jit) * np.float32(dx)).astype(np.float32)
+    rho = 1600.0
+    bed_vol = bed_cells[0] * bed_cells[1] * bed_cells[2] * dx ** 3
+    m = np.float32(rho * bed_vol / len(keep))
+    bed_top = bed_cells[1] * dx
+    s45 = math.sqrt(0.5)
+    wheel = Body(center=(0.3, bed_top + 0.1 - 0.01, 0.5), half_extents=(0.1, 0.04, 0.1),
+                 orientation=(s45, s45, 0.0, 0.0), linear_velocity=(0.1, 0.0, 0.0),
+                 angular_velocity=(0.0, 0.0, -2.0), friction=0.5, mass=5.0, shape=1, kinematic=True)
+    margin = 16
+    domain = ((-margin, -4, -margin), (grid + 2 * margin, bed_cells[1] + 40, grid + 2 * margin))
+    return Scene("wheel_rut", dx, grid, pos, np.full(len(keep), m, np.float32), 3.5e5, 0.3, rho,
+                 dp_alpha(30.0), 5e-5, 2000, bodies=[wheel], domain=domain)
+
+
+def scaled_wheel_rut(n_keep: int, seed=1) -> Scene:
+    """The wheel-rut scene with fewer particles kept (same bed and body)."""
+    return wheel_rut(n_keep=n_keep, seed=seed)
+
+
+def box_drop_scene(seed: int, grid: int | None = None, n_particles: int | None = None) -> Scene:
+    """One uneven batched scene: grid side in {32,48,64,96}, particle count
+    log-uniform 8k-400k at 8 ppc, friction angle U[25,40] deg, E log-uniform
+    [1e5, 1e6], a dynamic box of side U[0.05, 0.2] m with a random pose dropped
+    at U[0, 1] m/s."""
+    rng = np.random.default_rng(1000 + seed)
+    G = grid or int(rng.choice([32, 48, 64, 96]))
+    N = n_particles or int(math.exp(rng.uniform(math.log(8e3), math.log(4e5))))
+    dx = 1.0 / G
+    ppc = 8
+    cells = max(1, N // ppc)
+    # a sand block centred in x/z resting on the floor: width w x height h x w cells
+    w = max(2, min(G - 8, int(round((cells / 0.5) ** (1.0 / 3.0)))))
+    h = max(1, int(math.ceil(cells / (w * w))))
+    ncell = w * w * h
+    pos = np.empty((ncell * ppc, 3), np.float32)
+    ii, jj, kk = np.meshgrid(np.arange(w), np.arange(h), np.arange(w), indexing="ij")
+    base = np.stack([ii + (G - w) // 2, jj, kk + (G - w) // 2], -1).reshape(-1, 3).astype(np.float32)
+    jit = rng.random((ncell, ppc, 3), dtype=np.float32)
+    pos[:] = ((base[:, None, :] + jit) * np.float32(dx)).reshape(-1, 3)
+    pos = pos[:N]
+    rho = 1600.0
+    E = float(math.exp(rng.uniform(math.log(1e5), math.log(1e6))))
+    phi = float(rng.uniform(25.0, 40.0))
+    side = float(rng.uniform(0.05, 0.2))
+    q = rng.normal(size=4)
+    q = q / np.linalg.norm(q)
+    top = (h + 2) * dx
+    body = Body(center=(0.5, top + side, 0.5), half_extents=(side / 2,) * 3, orientation=tuple(map(float, q)),
+                linear_velocity=(0.0, -float(rng.uniform(0.0, 1.0)), 0.0), mass=float(rho * side ** 3),
+                shape=0, kinematic=False)
+    nu = 0.3
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    c = math.sqrt((lam + 2 * mu) / rho)
+    dt = min(2e-4, 0.5 * dx / c)
+    m = np.float32(rho * dx ** 3 / ppc)
+    return Scene(f"box_drop_{seed}", dx, G, pos, np.full(len(pos), m, np.float32), E, nu, rho, dp_alpha(phi),
+                 dt, 500, bodies=[body])

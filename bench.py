@@ -1,0 +1,355 @@
+#!/usr/bin/env python3
+"""Benchmark of the MLS-MPM soil step on B200: particle-steps/s.
+
+Workload (default): the plain large rigid-wheel rut, 2,000,000 particles on a
+128^3 grid (dx = 1/128) with the M1 PIC-rigid cylinder (R = 0.1 m, width
+0.08 m, 5 kg, 2 rad/s, 0.1 m/s), dt = 5e-5 s; one step = P2G, grid update,
+M1 coupler, G2P. Synthetic seeded inputs (no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun); the
+path has no inter-GPU exchange, so there is no collective on the data path.
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MPM particle-steps/s on 1 B200, batched+served vs plain; p50/p99 solve latency"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--particles", type=int, default=2_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# rank / process-group plumbing (replicas only: barrier + max over ranks)
+
+class Ranks:
+    def __init__(self, n_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.pg is None and self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def bytes_per_unit(n_particles: int, touched_nodes: int):
+    """Algorithmic bytes of one step (FP32 SoA): per particle 248 B (P2G reads
+    x,v,C,F,m,V0 = 26 floats; G2P reads x,F = 12 and writes x,v,C,F = 24) and
+    per touched node 80 B (P2G flush 7 floats, update reads 7 / writes 3, G2P
+    reads 3). Per kernel: P2G 104 B/particle + 28 B/node, grid update 40 B/node,
+    G2P 144 B/particle + 12 B/node."""
+    return {
+        "step": 248 * n_particles + 80 * touched_nodes,
+        "p2g": 104 * n_particles + 28 * touched_nodes,
+        "grid_update": 40 * touched_nodes,
+        "g2p": 144 * n_particles + 12 * touched_nodes,
+    }
+
+
+def run_ours(args, ranks: Ranks):
+    import basements_b200 as bm
+    from basements_b200 import scenes
+
+    if ranks.world > 1:
+        bm.set_device(ranks.local)
+    sc = scenes.wheel_rut(n_keep=args.particles)
+    body = sc.bodies[0]
+    s = bm.MPMSolver(sc.dx, domain=sc.domain)
+    s.set_material(sc.E, sc.nu, sc.rho)
+    s.set_plastic_alpha(sc.alpha)
+    s.add_particles(sc.position, None, sc.mass)
+
+    def collider(step):
+        return bm.make_collider(**body.at_time(step * sc.dt).as_tuple())
+
+    # warm-up (untimed)
+    for i in range(args.warmup):
+        s.step_coupled(sc.dt, [collider(i)], read_reactions=False)
+    st, _ = s.sync()
+    if st != 0:
+        raise RuntimeError(f"warm-up reported status {st}")
+    # touched nodes (for the algorithmic byte count)
+    s.p2g(sc.dt)
+    touched = int((s.get_grid()["mass"] > 0).sum())
+    s.grid_update(sc.dt)
+    s.g2p(sc.dt)
+    step0 = args.warmup + 1
+
+    # timed region: K coupled steps, inputs resident in HBM (208 MB of particle
+    # state, larger than the 126 MB L2), CUDA events on the solver's stream
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    idx = ranks.local if ranks.world > 1 else 0
+    sampler = ClockSampler(vis[idx] if idx < len(vis) and vis[idx] else str(idx))
+    s.profile(True)
+    s.profile_reset()
+    s.sync()
+    ranks.barrier()
+    sampler.start()
+    s.timer_start()
+    for i in range(args.steps):
+        s.step_coupled(sc.dt, [collider(step0 + i)], read_reactions=False)
+    ms = s.timer_stop()
+    clocks = sampler.stop()
+    ranks.barrier()
+    prof = s.profile_read()
+    st, esc = s.sync()
+    if st != 0:
+        raise RuntimeError(f"timed steps reported status {st} ({esc} escaped writes)")
+    ms_max = ranks.max(ms)
+    per_step_ms = ms_max / args.steps
+    value = sc.n * args.steps * ranks.world / (ms_max / 1e3)
+
+    # roofline of the dominant kernel
+    bpu = bytes_per_unit(sc.n, touched)
+    kernels = {k: v for k, v in prof.items() if v[1] > 0}
+    dom = max(kernels, key=lambda k: kernels[k][0])
+    dom_ms = kernels[dom][0] / kernels[dom][1]
+    peak, peak_kind = measured_peak_hbm()
+    alg = bpu.get(dom)
+    achieved = (alg / (dom_ms / 1e3)) / 1e9 if alg else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dom)
+    launches = sum(v[1] for k, v in kernels.items() if k != "grid_clear")
+    step_roof_gbs = bpu["step"] / (per_step_ms / 1e3) / 1e9
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded wheel-rut sand bed)",
+        "config": {"workload": "wheel_rut plain large rigid-wheel rut: 2M particles, 128^3 grid dx=1/128, "
+                               "M1 cylinder R=0.1 w=0.08 5kg, dt=5e-5",
+                   "particles": sc.n, "grid": sc.grid, "touched_nodes": touched,
+                   "parallelism": f"replicas{ranks.world}", "l2": "inputs larger than L2 (208 MB particle state)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "kernel_ms": dom_ms,
+                     "step_achieved_gbs": step_roof_gbs, "step_frac": step_roof_gbs / peak,
+                     "bytes_per_particle_step": bpu["step"] / sc.n},
+        "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in kernels.items()},
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+    }
+    s.close()
+    if not args.no_e2e:
+        out["e2e"] = run_e2e(args, sc, ranks)
+    return out
+
+
+def run_e2e(args, sc, ranks: Ranks):
+    """The same job through the public C ABI from host arrays: upload of the
+    particles, K coupled steps each taking the collider from the host and
+    returning the reaction to the host (synchronous), download of the final
+    positions and velocities."""
+    import basements_b200 as bm
+
+    body = sc.bodies[0]
+    colliders = [bm.make_collider(**body.at_time(i * sc.dt).as_tuple()) for i in range(args.steps)]
+    pos = np.ascontiguousarray(sc.position)
+    mass = np.ascontiguousarray(sc.mass)
+    # warm the library / context once outside the timed region
+    w = bm.MPMSolver(sc.dx, domain=sc.domain)
+    w.add_particles(pos[:1024], None, mass[:1024])
+    w.step_coupled(sc.dt, [colliders[0]])
+    w.close()
+    ranks.barrier()
+    t0 = time.perf_counter()
+    s = bm.MPMSolver(sc.dx, domain=sc.domain)
+    s.set_material(sc.E, sc.nu, sc.rho)
+    s.set_plastic_alpha(sc.alpha)
+    s.add_particles(pos, None, mass)
+    for i in range(args.steps):
+        s.step_coupled(sc.dt, [colliders[i]])
+    out = s.get_particles(("position", "velocity"))
+    el = time.perf_counter() - t0
+    s.close()
+    el = ranks.max(el)
+    n = sc.n
+    h2d = n * 16 + args.steps * 76
+    d2h = n * 24 + args.steps * 28
+    assert np.isfinite(out["position"]).all()
+    return {"value": n * args.steps * ranks.world / el, "unit": UNIT,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "what": "upload + K synchronous coupled steps (host collider in, host reaction out) + download"}
+
+
+def cpu_reference_rate(sc, n_steps: int, kind: str):
+    """Times the reference's own CPU MPMSolver (oracle/_ref, else the pinned
+    float restatement) on the wheel-rut scene: P2G, update_grid, M1 apply,
+    G2P per step, single thread (the reference has no threading)."""
+    from oracle import oracle as O
+
+    body = sc.bodies[0]
+    c = O.CpuSolver(kind, sc.dx)
+    c.set_material(sc.E, sc.nu, sc.rho)
+    c.set_plastic_alpha(sc.alpha)
+    c.add_particles(sc.position, None, sc.mass)
+    t0 = time.perf_counter()
+    for i in range(n_steps):
+        c.p2g(sc.dt)
+        c.grid_update(sc.dt)
+        c.m1_apply(O.collider(**body.at_time(i * sc.dt).as_tuple()), sc.dt)
+        c.g2p(sc.dt)
+    el = time.perf_counter() - t0
+    c.close()
+    return sc.n * n_steps / el, el
+
+
+def run_reference(args, ranks: Ranks):
+    from basements_b200 import scenes
+    from oracle import oracle as O
+
+    kind = O.reference_or_port()
+    sc = scenes.wheel_rut(n_keep=args.particles)
+    # each step is a bounded sample: the full 2M-particle coupled step (~3 s
+    # on one core); warm-up steps are not timed
+    n_timed = max(1, min(args.steps, 3))
+    n_warm = min(args.warmup, 1)
+    if n_warm:
+        cpu_reference_rate(sc, n_warm, kind)
+    rate, el = cpu_reference_rate(sc, n_timed, kind)
+    sample = f"{n_timed} coupled steps of the {sc.n}-particle wheel-rut scene"
+    cb = {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference" if kind == "ref" else "port",
+          "sample": sample}
+    return {"metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": ranks.world,
+            "steps": n_timed, "warmup": n_warm, "ms_per_step": el * 1e3 / n_timed, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded wheel-rut sand bed)",
+            "config": {"workload": "wheel_rut plain large rigid-wheel rut: 2M particles, 128^3 grid dx=1/128, "
+                                   "M1 cylinder R=0.1 w=0.08 5kg, dt=5e-5", "particles": sc.n,
+                       "parallelism": "1 host thread (the reference is single-threaded)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    ranks = Ranks(args.gpus)
+    try:
+        if args.impl == "reference":
+            if ranks.rank == 0:
+                print(json.dumps(run_reference(args, ranks)), flush=True)
+            return
+        out = run_ours(args, ranks)
+        if ranks.rank == 0 and not args.no_cpu_baseline:
+            from basements_b200 import scenes
+            from oracle import oracle as O
+            kind = O.reference_or_port()
+            if O.available(kind):
+                sc = scenes.wheel_rut(n_keep=args.particles)
+                rate, el = cpu_reference_rate(sc, 3, kind)
+                out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1,
+                                       "kind": "reference" if kind == "ref" else "port",
+                                       "sample": f"3 coupled steps of the {sc.n}-particle wheel-rut scene "
+                                                 f"({el:.1f} s, 1 thread)"}
+        if ranks.rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        ranks.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/* bm_mpm.h — C ABI of the B200-native MLS-MPM soil step.
+ *
+ * This is the drop-in boundary for the MPMSolver path of 2nugu/basements:
+ * plain pointers and sizes, no C++ or CUDA types in the signatures, every
+ * call returns a bm_status_t. One handle is driven by one host thread at a
+ * time; each handle owns a CUDA stream and its device buffers on the device
+ * that was current when it was created. Kernel work is enqueued on that
+ * stream; calls that return host data synchronise it.
+ *
+ * Reference interfaces replaced (paths inside 2nugu/basements):
+ *   MPMSolver               include/basements/physics/mpm/mpm_solver.h:15-95
+ *   Particle                include/basements/physics/mpm/particle.h:9-23
+ *   SPGridCPU / GridNode    include/basements/physics/mpm/spgrid_cpu.h:12-99
+ *   RigidColliderState      include/basements/physics/coupling/mpm_rigid_coupler.h:72-84
+ *   CouplingReaction        include/basements/physics/coupling/mpm_rigid_coupler.h:201-205
+ *   MPMRigidCouplerPIC      include/basements/physics/coupling/mpm_rigid_coupler_pic.h:88-184
+ *   ApplyFn (coupler table) research/mpm_rigid_coupling/bench_compare_all.cpp:50-51
+ *   TimeIntegrator          include/basements/physics/dynamics/integrator.h:19-57
+ *   plugin C-ABI idiom      include/basements/engine/plugins/plugin_capi.h:14-106
+ */
+#ifndef BM_MPM_H
+#define BM_MPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define BM_API __declspec(dllexport)
+#else
+#define BM_API __attribute__((visibility("default")))
+#endif
+
+#define BM_API_VERSION 1
+
+typedef enum bm_status {
+    BM_OK = 0,
+    BM_ERR_INVALID_ARGUMENT = 1, /* null handle, bad size, dx <= 0, ... */
+    BM_ERR_OUT_OF_MEMORY = 2,    /* device allocation failed or budget exceeded */
+    BM_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+    BM_ERR_DOMAIN_ESCAPE = 4,    /* a particle stencil left the dense grid box */
+    BM_ERR_NON_FINITE = 5,       /* NaN or Inf found in particle state */
+    BM_ERR_TIMEOUT = 6,          /* a bounded wait gave up */
+    BM_ERR_NOT_FOUND = 7,        /* unknown request or scene id */
+    BM_ERR_STATE = 8,            /* call out of order (e.g. g2p before p2g) */
+    BM_ERR_NO_DEVICE = 9         /* no CUDA device or the library was built without sm_100a */
+} bm_status_t;
+
+/* Dense grid box in node indices (node i sits at x = i*dx for the particle
+ * stencil; the floor test uses (j + 0.5)*dx like the reference). origin is
+ * rounded down and origin+extent up to multiples of 4 (the reference's 4^3
+ * block size, spgrid_cpu.h:38-40). */
+typedef struct bm_domain {
+    int32_t origin[3];
+    int32_t extent[3];
+} bm_domain_t;
+
+typedef enum bm_shape { BM_SHAPE_BOX = 0, BM_SHAPE_CYLINDER = 1 } bm_shape_t;
+
+/* Byte-for-byte the field meaning of RigidColliderState (mpm_rigid_coupler.h:72-84)
+ * with unpadded float[3]/float[4] in place of the 16-byte Vec3 / Quaternion.
+ * orientation is (w, x, y, z). CYLINDER: radius half_extents[0], half-length
+ * half_extents[1] along local Y. */
+typedef struct bm_collider {
+    float center[3];
+    float orientation[4];
+    float half_extents[3];
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float friction;
+    float mass;
+    int32_t shape;
+} bm_collider_t;
+
+/* CouplingReaction (mpm_rigid_coupler.h:201-205). */
+typedef struct bm_reaction {
+    float force[3];
+    float torque[3];
+    int32_t nodes_inside;
+} bm_reaction_t;
+
+/* Host SoA view of the particle store, one row per particle in the order the
+ * particles were added. Any pointer may be NULL to skip that field.
+ * Vectors are 3 floats, matrices 9 floats row-major (Particle, particle.h:9-23). */
+typedef struct bm_particles_view {
+    float* position;
+    float* velocity;
+    float* F;
+    float* C;
+    float* mass;
+    float* volume;
+} bm_particles_view_t;
+
+typedef struct bm_solver bm_solver_t;
+
+/* ---- library ---------------------------------------------------------- */
+BM_API int bm_get_version(void);
+BM_API const char* bm_status_string(bm_status_t status);
+/* Text of the last error raised on the calling thread (CUDA message, which argument). */
+BM_API const char* bm_last_error(void);
+/* Makes `device` current for the calling thread; handles created afterwards
+ * live on it (one process per GPU uses this with its local rank). */
+BM_API bm_status_t bm_set_device(int32_t device);
+
+/* ---- MPMSolver (mpm_solver.h:15-95) ----------------------------------- */
+/* MPMSolver() + initialize(dx) (:17-21). domain may be NULL: the box is then
+ * sized at the first step from the particle bounds plus `margin` nodes. */
+BM_API bm_status_t bm_solver_create(float dx, const bm_domain_t* domain, bm_solver_t** out);
+BM_API bm_status_t bm_solver_destroy(bm_solver_t* s);
+/* Sets the dense box explicitly (before the grid is first used). */
+BM_API bm_status_t bm_solver_set_domain(bm_solver_t* s, const bm_domain_t* domain);
+BM_API bm_status_t bm_solver_get_domain(bm_solver_t* s, bm_domain_t* out);
+/* Margin (nodes per side, default 16) used when the box is auto-sized. */
+BM_API bm_status_t bm_solver_set_auto_margin(bm_solver_t* s, int32_t margin_nodes);
+/* set_material (:42-51): rescales V0 of existing particles by rho_old / rho_new. */
+BM_API bm_status_t bm_solver_set_material(bm_solver_t* s, float young_modulus, float poisson_ratio,
+                                          float bulk_density);
+BM_API bm_status_t bm_solver_set_gravity(bm_solver_t* s, const float gravity[3]);      /* :52 */
+BM_API bm_status_t bm_solver_set_plastic_alpha(bm_solver_t* s, float alpha);           /* :53 */
+BM_API bm_status_t bm_solver_set_floor_friction(bm_solver_t* s, float mu_floor);       /* :54 */
+/* add_particle (:23-34) for n particles: V0 = m / rho, F = I, C = 0.
+ * velocity NULL means zero, mass NULL means 1.0 (the reference default). */
+BM_API bm_status_t bm_solver_add_particles(bm_solver_t* s, int64_t n, const float* position,
+                                           const float* velocity, const float* mass);
+BM_API bm_status_t bm_solver_num_particles(bm_solver_t* s, int64_t* out);
+/* get_particles (:89): device-to-host copy into the caller's SoA view. */
+BM_API bm_status_t bm_solver_get_particles(bm_solver_t* s, const bm_particles_view_t* view);
+/* get_particles_mutable (:59): overwrite fields of particles [first, first+n);
+ * NULL fields are left as they are. mass/volume are ignored. */
+BM_API bm_status_t bm_solver_set_particles(bm_solver_t* s, int64_t first, int64_t n,
+                                           const bm_particles_view_t* view);
+/* step(dt) (:62-87): clear, P2G, update_grid, G2P. Enqueued, returns at once. */
+BM_API bm_status_t bm_solver_step(bm_solver_t* s, float dt);
+/* n_steps plain steps, enqueued back to back. */
+BM_API bm_status_t bm_solver_step_n(bm_solver_t* s, float dt, int32_t n_steps);
+
+/* ---- split step + coupler plug-in (mpm_rigid_coupler.h:207-214) ------- */
+/* grid.clear() + the P2G loop (:72-78). */
+BM_API bm_status_t bm_solver_p2g(bm_solver_t* s, float dt);
+/* update_grid (:250-291). */
+BM_API bm_status_t bm_solver_grid_update(bm_solver_t* s, float dt);
+/* MPMRigidCouplerPIC::apply (mpm_rigid_coupler_pic.h:88-184): call between
+ * bm_solver_grid_update and bm_solver_g2p. dt <= 0 gives a zero reaction and
+ * leaves the grid unchanged. `out` is written before the call returns. */
+BM_API bm_status_t bm_coupler_m1_apply(bm_solver_t* s, const bm_collider_t* body, float dt,
+                                       bm_reaction_t* out);
+/* The G2P loop (:83-86). */
+BM_API bm_status_t bm_solver_g2p(bm_solver_t* s, float dt);
+/* P2G, grid update, M1 for each body in order, G2P, all on the handle's
+ * stream. reactions (n_bodies entries) may be NULL: the reactions then stay on
+ * the device until bm_solver_get_reactions. With a host pointer the call
+ * waits for the step to finish. */
+BM_API bm_status_t bm_solver_step_coupled(bm_solver_t* s, float dt, int32_t n_bodies,
+                                          const bm_collider_t* bodies, bm_reaction_t* reactions);
+BM_API bm_status_t bm_solver_get_reactions(bm_solver_t* s, int32_t n_bodies, bm_reaction_t* out);
+
+/* ---- grid access (get_grid / get_grid_mutable, :90-95) ----------------- */
+/* Number of nodes of the dense box (product of the rounded extents). */
+BM_API bm_status_t bm_solver_grid_num_nodes(bm_solver_t* s, int64_t* out);
+/* Dense copy in (i, j, k) order, k fastest, over the box of
+ * bm_solver_get_domain. Any pointer may be NULL. velocity holds what the
+ * reference's GridNode::velocity holds at this point of the step (momentum
+ * after P2G, velocity after update_grid). active is the reference's
+ * node.active: 1 for nodes touched this step. block_allocated (one byte per
+ * node) reports whether the node's 4^3 block has ever been touched, the
+ * blocks the reference's hash grid keeps (spgrid_cpu.h:78-91). */
+BM_API bm_status_t bm_solver_get_grid(bm_solver_t* s, float* velocity, float* force, float* mass,
+                                      uint8_t* active, uint8_t* block_allocated);
+/* Seeds nodes like the reference tests and scenarios do through get_node()
+ * (tests/test_mpm_rigid_coupler.cpp:30-34, scenario_box_drop.h:41-53): sets
+ * velocity and mass, marks each node active and its block allocated. Nodes
+ * outside the box are an error. */
+BM_API bm_status_t bm_solver_seed_grid(bm_solver_t* s, int64_t n, const int32_t* ijk, const float* velocity,
+                                       const float* mass);
+/* Overwrites the velocity of every node of the box from a dense array as
+ * returned by bm_solver_get_grid (mass is left as it is). */
+BM_API bm_status_t bm_solver_set_grid_velocity(bm_solver_t* s, const float* velocity);
+
+/* ---- status and diagnostics ------------------------------------------ */
+/* Waits for the handle's stream and returns the first device-side error
+ * seen since the last call (BM_ERR_DOMAIN_ESCAPE, BM_ERR_NON_FINITE), then
+ * clears it. escaped (may be NULL) gets the number of stencil writes dropped
+ * because they fell outside the box. */
+BM_API bm_status_t bm_solver_sync(bm_solver_t* s, int64_t* escaped);
+/* The CUDA stream (cudaStream_t) the handle enqueues on. */
+BM_API bm_status_t bm_solver_stream(bm_solver_t* s, void** stream);
+/* Per-kernel timing with CUDA events on the handle's stream (off by default).
+ * bm_solver_profile_read returns up to `cap` entries: name (static string),
+ * total milliseconds and launch count since the last reset. */
+BM_API bm_status_t bm_solver_profile_enable(bm_solver_t* s, int32_t on);
+BM_API bm_status_t bm_solver_profile_read(bm_solver_t* s, int32_t cap, const char** names, double* total_ms,
+                                          int64_t* launches, int32_t* n_out);
+BM_API bm_status_t bm_solver_profile_reset(bm_solver_t* s);
+/* Stream-ordered wall timer: records a CUDA event on the handle's stream at
+ * start; stop records a second one, waits for it and returns the elapsed
+ * milliseconds between the two. */
+BM_API bm_status_t bm_solver_timer_start(bm_solver_t* s);
+BM_API bm_status_t bm_solver_timer_stop(bm_solver_t* s, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BM_MPM_H */

@@ -1,0 +1,237 @@
+"""ctypes access to the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
+import this module. The product (``basements_b200``) never does.
+
+Three libraries export the interface of ``oracle/oracle_api.h``:
+
+* ``oracle/_ref/libref_mpm.so`` (prefix ``ref``): the reference's own
+  ``MPMSolver`` / ``MPMRigidCouplerPIC`` / ``TimeIntegrator`` compiled from its
+  headers by ``oracle/Makefile``;
+* ``oracle/liboracle_mpm_f32.so`` and ``liboracle_mpm_f64.so`` (prefix
+  ``orc``): the restatement in ``oracle/mpm_oracle.hpp`` in float and double.
+
+``CpuSolver`` mirrors the reference ``MPMSolver`` method names
+(include/basements/physics/mpm/mpm_solver.h:19-95) with numpy SoA arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+LIBS = {
+    "ref": os.path.join(HERE, "_ref", "libref_mpm.so"),
+    "f32": os.path.join(HERE, "liboracle_mpm_f32.so"),
+    "f64": os.path.join(HERE, "liboracle_mpm_f64.so"),
+}
+PREFIX = {"ref": "ref", "f32": "orc", "f64": "orc"}
+
+_f = C.POINTER(C.c_float)
+_i32 = C.POINTER(C.c_int32)
+_u8 = C.POINTER(C.c_uint8)
+
+
+class OrcCollider(C.Structure):
+    _fields_ = [
+        ("center", C.c_float * 3),
+        ("orientation", C.c_float * 4),
+        ("half_extents", C.c_float * 3),
+        ("linear_velocity", C.c_float * 3),
+        ("angular_velocity", C.c_float * 3),
+        ("friction", C.c_float),
+        ("mass", C.c_float),
+        ("shape", C.c_int32),
+    ]
+
+
+_loaded: dict = {}
+
+
+def available(kind: str) -> bool:
+    return os.path.exists(LIBS[kind])
+
+
+def load(kind: str):
+    """Load one checker library ("ref", "f32" or "f64")."""
+    if kind in _loaded:
+        return _loaded[kind]
+    path = LIBS[kind]
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built (run `make -C oracle`)")
+    lib = C.CDLL(path)
+    p = PREFIX[kind]
+
+    def fn(name, res, *args):
+        f = getattr(lib, f"{p}_{name}")
+        f.restype = res
+        f.argtypes = list(args)
+        return f
+
+    api = {
+        "precision_bytes": fn("precision_bytes", C.c_int),
+        "create": fn("create", C.c_void_p, C.c_float),
+        "destroy": fn("destroy", None, C.c_void_p),
+        "set_material": fn("set_material", None, C.c_void_p, C.c_float, C.c_float, C.c_float),
+        "set_gravity": fn("set_gravity", None, C.c_void_p, C.c_float, C.c_float, C.c_float),
+        "set_plastic_alpha": fn("set_plastic_alpha", None, C.c_void_p, C.c_float),
+        "set_floor_friction": fn("set_floor_friction", None, C.c_void_p, C.c_float),
+        "add_particles": fn("add_particles", None, C.c_void_p, C.c_int64, _f, _f, _f),
+        "num_particles": fn("num_particles", C.c_int64, C.c_void_p),
+        "set_particle_state": fn("set_particle_state", None, C.c_void_p, C.c_int64, C.c_int64, _f, _f, _f, _f),
+        "get_particles": fn("get_particles", None, C.c_void_p, _f, _f, _f, _f, _f, _f),
+        "step": fn("step", None, C.c_void_p, C.c_float, C.c_int),
+        "p2g": fn("p2g", None, C.c_void_p, C.c_float),
+        "grid_update": fn("grid_update", None, C.c_void_p, C.c_float),
+        "g2p": fn("g2p", None, C.c_void_p, C.c_float),
+        "m1_apply": fn("m1_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
+        "grid_num_nodes": fn("grid_num_nodes", C.c_int64, C.c_void_p),
+        "grid_get": fn("grid_get", C.c_int64, C.c_void_p, _i32, _f, _f, _f, _u8, C.c_int64),
+        "grid_seed": fn("grid_seed", None, C.c_void_p, C.c_int64, _i32, _f, _f),
+        "box_drop_m1": fn("box_drop_m1", C.c_int, _f, C.c_int),
+        "svd": fn("svd", None, C.c_int64, _f, _f, _f, _f),
+    }
+    _loaded[kind] = api
+    return api
+
+
+def _p(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_f)
+
+
+def collider(center, half_extents, orientation=(1.0, 0.0, 0.0, 0.0), linear_velocity=(0, 0, 0),
+             angular_velocity=(0, 0, 0), friction=0.5, mass=1.0, shape=0) -> OrcCollider:
+    c = OrcCollider()
+    c.center[:] = list(map(float, center))
+    c.orientation[:] = list(map(float, orientation))
+    c.half_extents[:] = list(map(float, half_extents))
+    c.linear_velocity[:] = list(map(float, linear_velocity))
+    c.angular_velocity[:] = list(map(float, angular_velocity))
+    c.friction = float(friction)
+    c.mass = float(mass)
+    c.shape = int(shape)
+    return c
+
+
+class CpuSolver:
+    """One CPU solver instance ("ref", "f32" or "f64")."""
+
+    def __init__(self, kind: str, dx: float):
+        self.kind = kind
+        self.api = load(kind)
+        self.h = self.api["create"](float(dx))
+
+    def close(self):
+        if self.h:
+            self.api["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference MPMSolver API --------------------------------------------
+    def set_material(self, E, nu, rho):
+        self.api["set_material"](self.h, E, nu, rho)
+
+    def set_gravity(self, g):
+        self.api["set_gravity"](self.h, *map(float, g))
+
+    def set_plastic_alpha(self, a):
+        self.api["set_plastic_alpha"](self.h, a)
+
+    def set_floor_friction(self, mu):
+        self.api["set_floor_friction"](self.h, mu)
+
+    def add_particles(self, pos, vel=None, mass=None):
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        mass = None if mass is None else np.ascontiguousarray(np.broadcast_to(np.float32(mass), (len(pos),)) if np.ndim(mass) == 0 else mass, np.float32)
+        self.api["add_particles"](self.h, len(pos), _p(pos), _p(vel), _p(mass))
+
+    def num_particles(self) -> int:
+        return int(self.api["num_particles"](self.h))
+
+    def set_particle_state(self, first=0, pos=None, vel=None, F=None, C_=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (pos, vel, F, C_)]
+        n = next(len(a.reshape(len(a), -1)) for a in arrs if a is not None)
+        self.api["set_particle_state"](self.h, first, n, *[_p(a) for a in arrs])
+
+    def get_particles(self):
+        n = self.num_particles()
+        out = {
+            "position": np.empty((n, 3), np.float32),
+            "velocity": np.empty((n, 3), np.float32),
+            "F": np.empty((n, 3, 3), np.float32),
+            "C": np.empty((n, 3, 3), np.float32),
+            "mass": np.empty(n, np.float32),
+            "volume": np.empty(n, np.float32),
+        }
+        self.api["get_particles"](self.h, *[_p(out[k]) for k in ("position", "velocity", "F", "C", "mass", "volume")])
+        return out
+
+    def step(self, dt, n_steps=1):
+        self.api["step"](self.h, dt, int(n_steps))
+
+    # -- split phases (coupler contract) -----------------------------------
+    def p2g(self, dt):
+        self.api["p2g"](self.h, dt)
+
+    def grid_update(self, dt):
+        self.api["grid_update"](self.h, dt)
+
+    def g2p(self, dt):
+        self.api["g2p"](self.h, dt)
+
+    def m1_apply(self, body: OrcCollider, dt):
+        r = np.zeros(6, np.float32)
+        n = self.api["m1_apply"](self.h, C.byref(body), dt, _p(r))
+        return r[:3].copy(), r[3:].copy(), int(n)
+
+    def grid_nodes(self):
+        """Every node of every allocated 4^3 block, as a dict keyed by (i,j,k)."""
+        cap = int(self.api["grid_num_nodes"](self.h))
+        ijk = np.empty((cap, 3), np.int32)
+        vel = np.empty((cap, 3), np.float32)
+        frc = np.empty((cap, 3), np.float32)
+        mass = np.empty(cap, np.float32)
+        act = np.empty(cap, np.uint8)
+        n = self.api["grid_get"](self.h, ijk.ctypes.data_as(_i32), _p(vel), _p(frc), _p(mass),
+                                 act.ctypes.data_as(_u8), cap)
+        return {"ijk": ijk[:n], "velocity": vel[:n], "force": frc[:n], "mass": mass[:n], "active": act[:n]}
+
+    def grid_seed(self, ijk, vel, mass):
+        ijk = np.ascontiguousarray(ijk, np.int32).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        mass = np.ascontiguousarray(mass, np.float32).reshape(-1)
+        self.api["grid_seed"](self.h, len(ijk), ijk.ctypes.data_as(_i32), _p(vel), _p(mass))
+
+
+def box_drop_m1(kind: str) -> np.ndarray:
+    api = load(kind)
+    rows = np.zeros((1000, 10), np.float32)
+    n = api["box_drop_m1"](_p(rows), 1000)
+    return rows[:n]
+
+
+def svd(kind: str, F: np.ndarray):
+    F = np.ascontiguousarray(F, np.float32).reshape(-1, 3, 3)
+    n = len(F)
+    U = np.empty_like(F)
+    V = np.empty_like(F)
+    S = np.empty((n, 3), np.float32)
+    load(kind)["svd"](n, _p(F), _p(U), _p(S), _p(V))
+    return U, S, V
+
+
+def reference_or_port() -> str:
+    """The strongest FP32 checker available: the compiled reference, else the
+    float restatement (pinned bit-exact to it by tests/test_oracle_pin.py)."""
+    return "ref" if available("ref") else "f32"

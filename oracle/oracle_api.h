@@ -1,0 +1,68 @@
+/* oracle_api.h — C interface shared by the two CPU checkers.
+ *
+ * TEST INFRASTRUCTURE ONLY (see mpm_oracle.hpp). Two libraries export this
+ * same set of functions under different prefixes:
+ *
+ *   orc_*  oracle/liboracle_mpm_f32.so and oracle/liboracle_mpm_f64.so —
+ *          the restatement in mpm_oracle.hpp, instantiated in float / double;
+ *   ref_*  oracle/_ref/libref_mpm.so — the reference's own MPMSolver,
+ *          MPMRigidCouplerPIC and TimeIntegrator compiled from its headers by
+ *          oracle/Makefile (never committed; rebuilt from the reference tree).
+ *
+ * All arrays are float at the boundary, particle data as SoA with 3 floats per
+ * vector and 9 row-major floats per matrix. The collider matches bm_collider_t.
+ */
+#ifndef BM_ORACLE_API_H
+#define BM_ORACLE_API_H
+#include <stdint.h>
+
+#ifndef ORACLE_PREFIX
+#error "define ORACLE_PREFIX (orc or ref) before including oracle_api.h"
+#endif
+#define ORC_CAT2(a, b) a##_##b
+#define ORC_CAT(a, b) ORC_CAT2(a, b)
+#define ORC(name) ORC_CAT(ORACLE_PREFIX, name)
+#define ORC_EXPORT extern "C" __attribute__((visibility("default")))
+
+typedef struct orc_collider {
+    float center[3];
+    float orientation[4]; /* w, x, y, z */
+    float half_extents[3];
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float friction;
+    float mass;
+    int32_t shape; /* 0 box, 1 cylinder */
+} orc_collider_t;
+
+ORC_EXPORT int ORC(precision_bytes)(void);
+ORC_EXPORT void* ORC(create)(float dx);
+ORC_EXPORT void ORC(destroy)(void* h);
+ORC_EXPORT void ORC(set_material)(void* h, float E, float nu, float rho);
+ORC_EXPORT void ORC(set_gravity)(void* h, float gx, float gy, float gz);
+ORC_EXPORT void ORC(set_plastic_alpha)(void* h, float a);
+ORC_EXPORT void ORC(set_floor_friction)(void* h, float mu);
+ORC_EXPORT void ORC(add_particles)(void* h, int64_t n, const float* pos, const float* vel, const float* mass);
+ORC_EXPORT int64_t ORC(num_particles)(void* h);
+ORC_EXPORT void ORC(set_particle_state)(void* h, int64_t first, int64_t n, const float* pos, const float* vel,
+                                       const float* F, const float* C);
+ORC_EXPORT void ORC(get_particles)(void* h, float* pos, float* vel, float* F, float* C, float* mass, float* vol);
+ORC_EXPORT void ORC(step)(void* h, float dt, int n_steps);
+ORC_EXPORT void ORC(p2g)(void* h, float dt);
+ORC_EXPORT void ORC(grid_update)(void* h, float dt);
+ORC_EXPORT void ORC(g2p)(void* h, float dt);
+/* reaction: force[3], torque[3]; returns nodes_inside */
+ORC_EXPORT int ORC(m1_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
+ORC_EXPORT int64_t ORC(grid_num_nodes)(void* h);
+/* every node of every allocated block; returns the count written (<= cap) */
+ORC_EXPORT int64_t ORC(grid_get)(void* h, int32_t* ijk, float* vel, float* force, float* mass, uint8_t* active,
+                                 int64_t cap);
+ORC_EXPORT void ORC(grid_seed)(void* h, int64_t n, const int32_t* ijk, const float* vel, const float* mass);
+/* The box_drop scene of the reference's research harness, method M1, grid
+ * only: 720 steps; per step 10 floats: t, box x/y/z, box vy, p_body_y,
+ * p_grid_y, p_sum_y, KE, nodes_inside. Returns the number of rows. */
+ORC_EXPORT int ORC(box_drop_m1)(float* rows, int max_rows);
+/* SVD of n row-major 3x3 matrices: U (n*9), sigma (n*3), V (n*9). */
+ORC_EXPORT void ORC(svd)(int64_t n, const float* F, float* U, float* S, float* V);
+
+#endif

@@ -1,0 +1,136 @@
+"""Parity of the CUDA M1 PIC-rigid coupler with the reference (GPU).
+
+* per-call fixtures made by the reference's MPMRigidCouplerPIC::apply on seeded
+  grids (boxes and cylinders, random poses, empty / tiny / normal node masses,
+  dt = 0): grid after the call and nodes_inside exactly, force and torque to
+  1e-5 relative (the reference sums in float in hash-map order, the kernel in
+  double per CTA);
+* the reference's grid-only box_drop scene (research harness, 720 steps)
+  against its shipped CSV;
+* a particle scene with a cylinder through bm_solver_step_coupled against the
+  reference's split phases P2G -> update_grid -> apply -> G2P.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import basements_b200 as bm
+from basements_b200 import scenes
+from oracle import oracle as O
+from tests.gpu_util import POS_TOL_100, cpu_solver, dense_index, gpu_solver, max_err_dx
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+REF = O.reference_or_port()
+
+pytestmark = pytest.mark.gpu
+
+
+def _body_from_row(b):
+    return dict(center=b[0:3], orientation=b[3:7], half_extents=b[7:10], linear_velocity=b[10:13],
+                angular_velocity=b[13:16], friction=float(b[16]), mass=float(b[17]), shape=int(b[18]))
+
+
+def test_m1_matches_reference_fixtures():
+    d = np.load(os.path.join(GOLD, "m1_cases.npz"))
+    off = {k: np.concatenate([[0], np.cumsum(d[k + "_len"])]) for k in ("seed_ijk", "grid_ijk")}
+    for c in range(len(d["dx"])):
+        sl = slice(off["seed_ijk"][c], off["seed_ijk"][c + 1])
+        ijk = d["seed_ijk"][sl]
+        lo = ijk.min(0) - 8
+        hi = ijk.max(0) + 8
+        s = bm.MPMSolver(float(d["dx"][c]), domain=(tuple(lo), tuple(hi - lo)))
+        s.seed_grid(ijk, d["seed_vel"][sl], d["seed_mass"][sl])
+        body = bm.make_collider(**_body_from_row(d["body"][c]))
+        f, t, n = s.m1_apply(body, float(d["dt"][c]))
+        assert n == d["nodes_inside"][c], c
+        fr, tr = d["force"][c], d["torque"][c]
+        scale = max(np.abs(fr).max(), 1e-30)
+        assert np.abs(f - fr).max() <= 1e-5 * scale + 1e-30, (c, f, fr)
+        assert np.abs(t - tr).max() <= 1e-5 * max(np.abs(tr).max(), 1e-30) + 1e-30, (c, t, tr)
+        g = s.get_grid()
+        gs = slice(off["grid_ijk"][c], off["grid_ijk"][c + 1])
+        idx = dense_index(g, d["grid_ijk"][gs])
+        assert np.array_equal(g["velocity"].reshape(-1, 3)[idx], d["grid_vel"][gs])
+        assert np.array_equal(g["mass"].reshape(-1)[idx], d["grid_mass"][gs])
+        # nodes of blocks the reference never allocated stay empty
+        mask = np.ones(g["mass"].size, bool)
+        mask[idx] = False
+        assert np.all(g["mass"].reshape(-1)[mask] == 0)
+
+
+def _quat_mul(a, b):
+    f = np.float32
+    aw, ax, ay, az = a
+    bw, bx, by, bz = b
+    return (f(f(f(aw * bw) - f(ax * bx)) - f(ay * by)) - f(az * bz),
+            f(f(f(aw * bx) + f(ax * bw)) + f(ay * bz)) - f(az * by),
+            f(f(f(aw * by) - f(ax * bz)) + f(ay * bw)) + f(az * bx),
+            f(f(f(aw * bz) + f(ax * by)) - f(ay * bx)) + f(az * bw))
+
+
+def test_box_drop_scene_matches_reference_csv():
+    """research/mpm_rigid_coupling/bench_compare_all.cpp:72-208, M1: the
+    harness loop runs here in float32 numpy around the CUDA coupler."""
+    gold = np.load(os.path.join(GOLD, "box_drop_M1.npz"))
+    f = np.float32
+    dx, dt, g, mass = f(0.1), f(1.0 / 240.0), f(9.81), f(1.0)
+    s = bm.MPMSolver(0.1, domain=((-8, -4, -8), (16, 16, 16)))
+    ijk = np.array([(i, j, k) for i in range(-3, 4) for j in range(3) for k in range(-3, 4)], np.int32)
+    s.seed_grid(ijk, np.zeros((len(ijk), 3), np.float32), np.full(len(ijk), 0.01, np.float32))
+    pos = np.array([0, 0.55, 0], np.float32)
+    vel = np.zeros(3, np.float32)
+    omg = np.zeros(3, np.float32)
+    q = (f(1), f(0), f(0), f(0))
+    rows = []
+    for i in range(len(gold["rows"])):
+        force = np.array([0, -g * mass, 0], np.float32)
+        body = bm.make_collider(pos, (0.2, 0.2, 0.2), q, vel, omg, 0.5, 1.0, 0)
+        fr, tq, n = s.m1_apply(body, float(dt))
+        force = (force + fr).astype(np.float32)
+        vel = (vel + (force * (f(1) / mass)) * dt).astype(np.float32)
+        omg = (omg + tq.astype(np.float32) * dt).astype(np.float32)
+        pos = (pos + vel * dt).astype(np.float32)
+        dq = _quat_mul((f(0), omg[0], omg[1], omg[2]), q)
+        h = f(f(0.5) * dt)
+        q = tuple(f(q[a] + f(dq[a] * h)) for a in range(4))
+        nrm = f(np.sqrt(f(f(f(q[0] * q[0]) + f(q[1] * q[1])) + f(q[2] * q[2])) + f(q[3] * q[3])))
+        q = tuple(f(c * f(f(1) / nrm)) for c in q)
+        grid = s.get_grid()
+        v = grid["velocity"].copy()
+        act = grid["mass"] > 0
+        vy = v[..., 1]
+        vy[act] = vy[act] + (-g * dt)
+        vy[act & (vy < 0)] = 0
+        s.set_grid_velocity(v)
+        pg = (v[act] * grid["mass"][act][:, None]).astype(np.float64).sum(0)
+        pb = vel * mass
+        rows.append([pos[0], pos[1], pos[2], vel[1], pb[1], pg[1], pb[1] + pg[1], n])
+    rows = np.array(rows)
+    ref = gold["rows"]
+    np.testing.assert_allclose(rows[:, 0:3], ref[:, 1:4], atol=2e-5)
+    np.testing.assert_allclose(rows[:, 3], ref[:, 4], atol=2e-4)
+    assert np.array_equal(rows[:, 7], ref[:, 9])
+    names = list(gold["metric_names"])
+    max_p = np.abs(rows[:, 6]).max()
+    assert abs(max_p - gold["metric_values"][names.index("max_abs_total_p_y")]) < 1e-4 * 0.18
+
+
+def test_coupled_particle_scene_matches_reference_split():
+    sc = scenes.wheel_rut(n_keep=20000)
+    body = sc.bodies[0]
+    g = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha, domain=sc.domain)
+    c = cpu_solver(REF, sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+    for n in range(40):
+        b = body.at_time(n * sc.dt)
+        gr = g.step_coupled(sc.dt, [bm.make_collider(**b.as_tuple())])[0]
+        c.p2g(sc.dt)
+        c.grid_update(sc.dt)
+        cr = c.m1_apply(O.collider(**b.as_tuple()), sc.dt)
+        c.g2p(sc.dt)
+        assert gr[2] == cr[2]
+        np.testing.assert_allclose(gr[0], cr[0], rtol=1e-3, atol=1e-3 * max(1.0, np.abs(cr[0]).max()))
+    e = max_err_dx(g.get_particles()["position"], c.get_particles()["position"], sc.dx)
+    print(f"coupled wheel scene, 40 steps: max |x_gpu - x_ref| = {e:.3e} dx")
+    assert e <= POS_TOL_100
+    assert g.sync() == (0, 0)

@@ -1,0 +1,196 @@
+"""Parity of the CUDA plain step with the reference (GPU).
+
+Checkers: the reference compiled from its headers (oracle/_ref) when built,
+else the float restatement pinned bit-exact to it; the FP64 restatement; and
+the committed fixtures made by the reference. Accuracy bars: particle
+positions within 1e-4*dx after 100 steps and 1e-3*dx after 1000 steps of the
+16,384-particle sand column; grid mass equal to the particle mass to 1e-6
+relative. FP32 atomics make the P2G sums order-dependent, so two GPU runs may
+differ in the last bits; the bound is checked too.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import basements_b200 as bm
+from basements_b200 import scenes
+from oracle import oracle as O
+from tests.gpu_util import (MASS_REL_TOL, POS_TOL_100, POS_TOL_1000, cpu_solver, dense_index, gpu_solver,
+                            max_err_dx, scene_solvers)
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+REF = O.reference_or_port()
+
+pytestmark = pytest.mark.gpu
+
+
+def test_small_scene_phases_match_reference_fixture():
+    d = np.load(os.path.join(GOLD, "small_scene.npz"))
+    dx = float(d["dx"])
+    s = gpu_solver(dx, d["pos0"], d["vel0"], d["mass"], 3.5e5, 0.3, 1600.0, float(d["alpha"]))
+    s.p2g(1e-4)
+    g = s.get_grid()
+    idx = dense_index(g, d["p2g_ijk"])
+    m = g["mass"].reshape(-1)[idx]
+    np.testing.assert_allclose(m, d["p2g_mass"], rtol=1e-5, atol=1e-12)
+    mom = g["velocity"].reshape(-1, 3)[idx]
+    scale = np.abs(d["p2g_vel"]).max()
+    assert np.abs(mom - d["p2g_vel"]).max() <= 1e-5 * scale
+    frc = g["force"].reshape(-1, 3)[idx]
+    assert np.abs(frc - d["p2g_force"]).max() <= 1e-5 * np.abs(d["p2g_force"]).max()
+    # nodes outside the reference's allocated blocks hold nothing
+    mask = np.ones(g["mass"].size, bool)
+    mask[idx] = False
+    assert np.all(g["mass"].reshape(-1)[mask] == 0)
+    # same allocated blocks
+    assert np.all(g["block_allocated"].reshape(-1)[idx] == 1)
+    assert g["block_allocated"].sum() == len(idx)
+    s.grid_update(1e-4)
+    g = s.get_grid()
+    idx = dense_index(g, d["upd_ijk"])
+    v = g["velocity"].reshape(-1, 3)[idx]
+    assert np.abs(v - d["upd_vel"]).max() <= 1e-5 * np.abs(d["upd_vel"]).max()
+    s.g2p(1e-4)
+    s.step(1e-4, 19)
+    p = s.get_particles()
+    assert max_err_dx(p["position"], d["pos20"], dx) < POS_TOL_100
+    np.testing.assert_allclose(p["F"], d["F20"], atol=1e-5)
+    assert s.sync() == (0, 0)
+
+
+def test_mass_conservation_after_p2g():
+    sc = scenes.sand_column()
+    s = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+    s.step(sc.dt, 50)
+    s.p2g(sc.dt)
+    grid_mass = s.get_grid()["mass"].astype(np.float64).sum()
+    pm = s.get_particles(("mass",))["mass"].astype(np.float64).sum()
+    assert abs(grid_mass - pm) / pm < MASS_REL_TOL
+
+
+def test_sand_column_100_and_1000_steps():
+    sc = scenes.sand_column()
+    g, c = scene_solvers(sc, REF)
+    f64 = cpu_solver("f64", sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+    g.step(sc.dt, 100)
+    c.step(sc.dt, 100)
+    f64.step(sc.dt, 100)
+    pg = g.get_particles()
+    pc = c.get_particles()
+    e100 = max_err_dx(pg["position"], pc["position"], sc.dx)
+    e100_64 = max_err_dx(pg["position"], f64.get_particles()["position"], sc.dx)
+    print(f"sand column 100 steps: max |x_gpu - x_ref| = {e100:.3e} dx, vs FP64 {e100_64:.3e} dx")
+    assert e100 <= POS_TOL_100 and e100_64 <= POS_TOL_100
+    np.testing.assert_allclose(pg["velocity"], pc["velocity"], atol=1e-4)
+    g.step(sc.dt, 900)
+    c.step(sc.dt, 900)
+    e1000 = max_err_dx(g.get_particles()["position"], c.get_particles()["position"], sc.dx)
+    print(f"sand column 1000 steps: max |x_gpu - x_ref| = {e1000:.3e} dx")
+    assert e1000 <= POS_TOL_1000
+    assert g.sync() == (0, 0)
+
+
+def test_two_runs_agree_within_atomic_order_bound():
+    sc = scenes.sand_column()
+    runs = []
+    for _ in range(2):
+        s = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+        s.step(sc.dt, 100)
+        runs.append(s.get_particles()["position"])
+    assert max_err_dx(runs[0], runs[1], sc.dx) < 1e-5
+
+
+def test_reference_unit_tests_on_gpu():
+    """tests/test_mpm_constitutive.cpp, test_mpm_stress_isolation.cpp and
+    test_mpm_cpu.cpp restated through the CUDA library, and compared with the
+    reference's own outputs for the same cases."""
+    c = np.load(os.path.join(GOLD, "constitutive.npz"))
+
+    def single(F=None, positions=((0.2, 0.2, 0.2),), alpha=None):
+        s = gpu_solver(0.1, np.array(positions, np.float32), None, np.full(len(positions), 0.01, np.float32),
+                       1e5, 0.3, 1500.0, alpha, gravity=(0, 0, 0))
+        if F is not None:
+            s.set_particles(0, F=np.array(F, np.float32))
+        s.step(1.0 / 240.0)
+        return s
+
+    def speed(s):
+        g = s.get_grid()
+        v = g["velocity"][g["active"] > 0]
+        return float(np.linalg.norm(v, axis=1).max())
+
+    assert speed(single()) < 1e-6
+    v1 = speed(single([np.diag([1, 1.005, 1])]))
+    v2 = speed(single([np.diag([1, 1.01, 1])]))
+    assert v1 > 1e-8 and abs(v2 / v1 - 2.0) < 0.14
+    np.testing.assert_allclose([v1, v2], [c["strain_0.005_speed"], c["strain_0.01_speed"]], rtol=1e-5)
+    F = single([np.diag([1.5, 0.5, 1.5])], alpha=0.6).get_particles()["F"][0]
+    np.testing.assert_allclose(F, c["dp_F"], atol=1e-5)
+    v = single([np.diag([1, 0.9, 1])] * 2, positions=((0.2, 0.18, 0.2), (0.2, 0.22, 0.2))).get_particles()["velocity"]
+    assert v[0, 1] < -1e-4 and v[1, 1] > 1e-4 and np.all(np.abs(v[:, [0, 2]]) < 1e-4)
+    np.testing.assert_allclose(v, c["column_vel"], rtol=1e-4, atol=1e-7)
+    cc, o = 0.3, 0.02
+    pts = ((cc - o, cc, cc), (cc + o, cc, cc), (cc, cc - o, cc), (cc, cc + o, cc), (cc, cc, cc - o), (cc, cc, cc + o))
+    v = single([np.eye(3) * 0.95] * 6, positions=pts).get_particles()["velocity"]
+    np.testing.assert_allclose(v, c["hydro_vel"], rtol=1e-4, atol=1e-7)
+    # test_mpm_cpu.cpp: lattice column (fract == 0 exactly -> zero weights skipped)
+    xs = np.arange(0.5, 1.0 - 1e-6, 0.05, dtype=np.float32)
+    pts = np.array([(x, y, z) for x in xs for y in xs for z in xs], np.float32)
+    s = bm.MPMSolver(0.1)
+    s.add_particles(pts)
+    ref = O.CpuSolver(REF, 0.1)
+    ref.add_particles(pts)
+    s.step(0.01, 10)
+    ref.step(0.01, 10)
+    py = s.get_particles()["position"]
+    assert py[:, 1].mean() < 0.74
+    assert max_err_dx(py, ref.get_particles()["position"], 0.1) < POS_TOL_100
+    s = bm.MPMSolver(0.1)
+    s.add_particles(np.array([[0.5, 0.05, 0.5]], np.float32), np.array([[0, -10.0, 0]], np.float32))
+    s.step(0.01, 10)
+    assert s.get_particles()["position"][0, 1] >= 0.0
+
+
+def test_set_material_rescales_volume_like_reference():
+    pos = np.array([[0.2, 0.2, 0.2], [0.3, 0.25, 0.2]], np.float32)
+    s = bm.MPMSolver(0.1)
+    s.add_particles(pos, None, [0.01, 0.02])
+    s.set_material(2e5, 0.25, 1800.0)
+    r = O.CpuSolver(REF, 0.1)
+    r.add_particles(pos, None, np.array([0.01, 0.02], np.float32))
+    r.set_material(2e5, 0.25, 1800.0)
+    assert np.array_equal(s.get_particles()["volume"], r.get_particles()["volume"])
+
+
+def test_edge_cases():
+    # empty store with an explicit box: steps are no-ops
+    s = bm.MPMSolver(0.1, domain=((-4, -4, -4), (8, 8, 8)))
+    s.step(0.01, 3)
+    assert s.num_particles() == 0 and s.sync() == (0, 0)
+    # particles resting on y = 0 use nodes j = -1 (base_y = floor(-0.5) = -1)
+    pos = np.array([[0.5, 0.0, 0.5], [0.52, 1e-7, 0.5]], np.float32)
+    s = bm.MPMSolver(0.1)
+    s.add_particles(pos, [[0.1, -1.0, 0.0]] * 2, 0.01)
+    r = O.CpuSolver(REF, 0.1)
+    r.add_particles(pos, np.array([[0.1, -1.0, 0.0]] * 2, np.float32), np.full(2, 0.01, np.float32))
+    s.step(0.01, 5)
+    r.step(0.01, 5)
+    assert max_err_dx(s.get_particles()["position"], r.get_particles()["position"], 0.1) < POS_TOL_100
+    # a box too small for the motion: escape is reported, nothing is written out of bounds
+    s = bm.MPMSolver(0.1, domain=((0, 0, 0), (4, 4, 4)))
+    s.add_particles(np.array([[0.2, 0.2, 0.2]], np.float32), [[50.0, 0, 0]], 0.01)
+    s.step(0.01, 3)
+    st, esc = s.sync()
+    assert st == 4 and esc > 0
+    # non-finite state is reported
+    s = bm.MPMSolver(0.1, domain=((-4, -4, -4), (16, 16, 16)))
+    s.add_particles(np.array([[0.2, 0.2, 0.2]], np.float32))
+    s.set_particles(0, F=np.full((1, 3, 3), np.nan, np.float32))
+    s.step(0.01)
+    assert s.sync()[0] == 5
+    # argument validation
+    with pytest.raises(bm.BMError):
+        s.step(float("nan"))
+    with pytest.raises(bm.BMError):
+        s.set_particles(5, position=np.zeros((1, 3), np.float32))
