@@ -73,6 +73,8 @@ _SIGS = {
     "bm_solver_set_domain": (_st, [_h, C.POINTER(Domain)]),
     "bm_solver_get_domain": (_st, [_h, C.POINTER(Domain)]),
     "bm_solver_set_auto_margin": (_st, [_h, C.c_int32]),
+    "bm_solver_set_sort_interval": (_st, [_h, C.c_int32]),
+    "bm_solver_set_math_mode": (_st, [_h, C.c_int32]),
     "bm_solver_set_material": (_st, [_h, C.c_float, C.c_float, C.c_float]),
     "bm_solver_set_gravity": (_st, [_h, _f]),
     "bm_solver_set_plastic_alpha": (_st, [_h, C.c_float]),
@@ -192,6 +194,12 @@ class MPMSolver:
     @property
     def handle(self):
         return self._h
+
+    def set_sort_interval(self, steps: int):
+        check(lib().bm_solver_set_sort_interval(self._h, int(steps)), "bm_solver_set_sort_interval")
+
+    def set_math_mode(self, fast: bool):
+        check(lib().bm_solver_set_math_mode(self._h, 1 if fast else 0), "bm_solver_set_math_mode")
 
     # -- MPMSolver API (mpm_solver.h:19-95) -----------------------------------
     def set_material(self, young_modulus, poisson_ratio, bulk_density):

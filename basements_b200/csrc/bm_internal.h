@@ -10,7 +10,7 @@
 
 namespace bm {
 
-// Device-side error bits, OR-ed into Solver::d_status[0].
+// Device-side error bits, OR-ed into the solver's status word.
 enum : uint32_t { ERR_ESCAPE = 1u, ERR_NONFINITE = 2u };
 
 // Particle planes of the SoA store (each plane holds `cap` floats).
@@ -24,24 +24,46 @@ enum Plane : int {
     N_PLANES = 26
 };
 
-// Dense grid box, blocked in 4^3-node blocks aligned to absolute node
-// indices (the reference's block grid, spgrid_cpu.h:93-105). Node (i,j,k)
-// lives at block ((i-ox)>>2, (j-oy)>>2, (k-oz)>>2) and local slot
-// (i&3)*16 + (j&3)*4 + (k&3).
+// Dense grid box: nodes stored x-major with k fastest (node (i,j,k) at
+// ((i-ox)*EY + (j-oy))*EZ + (k-oz)), so the 27 stencil nodes of a particle
+// sit at constant offsets from its base node. The box is a whole number of
+// 4^3-node blocks aligned to absolute node indices (the reference's block
+// grid, spgrid_cpu.h:93-105); per-block flags (allocated, touched) use block
+// (bi,bj,bk) = ((i-ox)>>2, (j-oy)>>2, (k-oz)>>2), local slot li*16+lj*4+lk.
 struct GridDesc {
     int ox, oy, oz;       // origin node, multiple of 4
     int nbx, nby, nbz;    // blocks per axis
     float dx, inv_dx;
+    __host__ __device__ int ex() const { return nbx * 4; }
+    __host__ __device__ int ey() const { return nby * 4; }
+    __host__ __device__ int ez() const { return nbz * 4; }
     __host__ __device__ int64_t num_blocks() const { return (int64_t)nbx * nby * nbz; }
     __host__ __device__ int64_t num_nodes() const { return num_blocks() * 64; }
+    __host__ __device__ __forceinline__ int64_t block_of(int bi, int bj, int bk) const {
+        return ((int64_t)bi * nby + bj) * nbz + bk;
+    }
+    // Node index from box-relative coordinates (no check).
+    __host__ __device__ __forceinline__ int64_t node_rel(int ri, int rj, int rk) const {
+        return ((int64_t)ri * (nby * 4) + rj) * (nbz * 4) + rk;
+    }
     // Linear node index, or -1 outside the box.
     __host__ __device__ __forceinline__ int64_t node(int i, int j, int k) const {
         const int ri = i - ox, rj = j - oy, rk = k - oz;
         if ((unsigned)ri >= (unsigned)(nbx * 4) || (unsigned)rj >= (unsigned)(nby * 4) ||
             (unsigned)rk >= (unsigned)(nbz * 4))
             return -1;
-        const int64_t b = ((int64_t)(ri >> 2) * nby + (rj >> 2)) * nbz + (rk >> 2);
-        return b * 64 + ((ri & 3) * 16 + (rj & 3) * 4 + (rk & 3));
+        return node_rel(ri, rj, rk);
+    }
+    // Node of block b at local slot t = li*16 + lj*4 + lk.
+    __host__ __device__ __forceinline__ int64_t node_of_block(int64_t b, int t) const {
+        const int bk = (int)(b % nbz), bj = (int)((b / nbz) % nby), bi = (int)(b / ((int64_t)nbz * nby));
+        return node_rel(4 * bi + (t >> 4), 4 * bj + ((t >> 2) & 3), 4 * bk + (t & 3));
+    }
+    // Block of a linear node index.
+    __host__ __device__ __forceinline__ int64_t block_of_node(int64_t id) const {
+        const int64_t ez_ = nbz * 4, ey_ = nby * 4;
+        const int rk = (int)(id % ez_), rj = (int)((id / ez_) % ey_), ri = (int)(id / (ez_ * ey_));
+        return block_of(ri >> 2, rj >> 2, rk >> 2);
     }
 };
 
@@ -56,23 +78,81 @@ struct Material {
 
 struct ParticleSoA {
     float* base;   // N_PLANES planes of `cap` floats
+    int32_t* pid;  // add-order index of each stored particle
     int64_t cap;
     int64_t n;
     __host__ __device__ __forceinline__ float* plane(int p) const { return base + (int64_t)p * cap; }
 };
 
-struct GridBuffers {
-    float4* mv;      // momentum (after update: velocity) xyz, mass w
-    float4* f;       // force xyz
-    uint8_t* alloc;  // per block: ever touched
+// One accumulation buffer of the grid: (momentum -> velocity, mass) and
+// (force, 0) per node, plus the list of blocks that hold non-zero data.
+struct GridAcc {
+    float4* mv;
+    float4* f;
+    uint32_t* touched;  // per block: listed in `list`
+    int32_t* list;      // touched block ids
+    int32_t* count;     // number of entries in `list`
 };
 
-// Kernel launchers (bm_step_kernels.cu, bm_m1.cu).
-void launch_p2g(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat, float dt,
+struct GridBuffers {
+    GridAcc acc;        // the buffer a kernel reads / updates
+    uint8_t* alloc;     // per block: ever touched (the reference's allocated blocks)
+};
+
+// Marks block b as holding data in `a` (appends it to the list once).
+__device__ __forceinline__ void touch_block(const GridAcc& a, int64_t b) {
+    if (a.touched[b] == 0u && atomicExch(a.touched + b, 1u) == 0u) a.list[atomicAdd(a.count, 1)] = (int32_t)b;
+}
+
+// Marks the 4^3 blocks covered by the stencil nodes of non-zero 1-D weight
+// (base..base+2 per axis, the end nodes dropped when their weight is 0) as
+// allocated (the reference allocates a block on the first get_node() of any
+// node in it, spgrid_cpu.h:78-91) and as holding data in `a`.
+__device__ __forceinline__ void mark_stencil_blocks(const GridDesc& g, const GridAcc& a, uint8_t* alloc,
+                                                    const int base[3], const float wx[3], const float wy[3],
+                                                    const float wz[3]) {
+    const int lo0 = base[0] + (wx[0] == 0.0f), hi0 = base[0] + 2 - (wx[2] == 0.0f);
+    const int lo1 = base[1] + (wy[0] == 0.0f), hi1 = base[1] + 2 - (wy[2] == 0.0f);
+    const int lo2 = base[2] + (wz[0] == 0.0f), hi2 = base[2] + 2 - (wz[2] == 0.0f);
+    for (int i = (lo0 - g.ox) >> 2; i <= (hi0 - g.ox) >> 2; ++i)
+        for (int j = (lo1 - g.oy) >> 2; j <= (hi1 - g.oy) >> 2; ++j)
+            for (int k = (lo2 - g.oz) >> 2; k <= (hi2 - g.oz) >> 2; ++k) {
+                if ((unsigned)i < (unsigned)g.nbx && (unsigned)j < (unsigned)g.nby && (unsigned)k < (unsigned)g.nbz) {
+                    const int64_t blk = g.block_of(i, j, k);
+                    if (alloc[blk] == 0) alloc[blk] = 1;
+                    touch_block(a, blk);
+                }
+            }
+}
+
+// Kernel launchers (bm_step_kernels.cu): the split phases.
+void launch_p2g(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat,
                 uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st);
-void launch_grid_update(const GridDesc& g, const GridBuffers& gb, const Material& mat, float dt, cudaStream_t st);
+// folded: cur.mv holds momentum + force * dt (the force channel only holds
+// the contributions of w*m <= 1e-6 particle-node pairs).
+void launch_grid_update(const GridDesc& g, const GridAcc& cur, const GridAcc& other, const Material& mat, float dt,
+                        bool folded, int64_t max_blocks, cudaStream_t st);
 void launch_g2p(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat, float dt,
                 uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st);
+
+// Particle ordering and fused G2P + next P2G (bm_fused.cu). Particles are
+// sorted by their stencil base node (key = flat node index of
+// floor(x/dx - 0.5); nkeys = num_nodes is the "outside the box" key).
+struct BinBuffers {
+    int32_t* key;        // per particle: key
+    int32_t* rank;       // per particle: slot among particles with the same key
+    int32_t* count;      // nkeys + 1
+    int32_t* start;      // nkeys + 2 (exclusive scan)
+    int64_t* tile_sum;   // per scan tile
+    int64_t nkeys;       // real keys (= grid nodes)
+    int64_t key_cap;     // capacity of key / rank
+};
+int64_t scan_tiles(int64_t nkeys);
+void launch_bin_sort(const ParticleSoA& src, const ParticleSoA& dst, const GridDesc& g, const BinBuffers& bb,
+                     cudaStream_t st);
+void launch_g2p2g(const ParticleSoA& ps, const GridDesc& g, const GridAcc& cur, const GridAcc& next,
+                  uint8_t* alloc, const Material& mat, float dt, float dt_next, bool fast_math,
+                  uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st);
 
 // M1 PIC-rigid coupler; accumulates into d_acc (6 doubles + 1 count as double).
 struct M1Params {
@@ -95,6 +175,12 @@ void launch_grid_to_dense(const GridDesc& g, const GridBuffers& gb, float* vel, 
 void launch_dense_velocity_to_grid(const GridDesc& g, const GridBuffers& gb, const float* vel, cudaStream_t st);
 void launch_seed_grid(const GridDesc& g, const GridBuffers& gb, int64_t n, const int32_t* ijk, const float* vel,
                       const float* mass, uint32_t* d_status, cudaStream_t st);
+
+// Particle rows in add order <-> stored order.
+void launch_gather_rows(const ParticleSoA& ps, int plane0, int width, float* out_add_order, cudaStream_t st);
+void launch_scatter_rows(const ParticleSoA& ps, int plane0, int width, const float* in_rows, int64_t first,
+                         int64_t n, const int32_t* inv, cudaStream_t st);
+void launch_inverse_pid(const ParticleSoA& ps, int32_t* inv, cudaStream_t st);
 
 // Thread-local error text.
 void set_last_error(const std::string& s);

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params 
     }
     if (visit) {
         const int li = t >> 4, lj = (t >> 2) & 3, lk = t & 3;
-        const int64_t id = blin * 64 + t;
+        const int64_t id = g.node_of_block(blin, t);
         const float xn[3] = {mul((float)(ox + li) + 0.5f, dx), mul((float)(oy + lj) + 0.5f, dx),
                              mul((float)(oz + lk) + 0.5f, dx)};
         const float r[3] = {sub(xn[0], P.c[0]), sub(xn[1], P.c[1]), sub(xn[2], P.c[2])};
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params 
             const float vb[3] = {add(P.vl[0], sub(mul(P.w[1], r[2]), mul(P.w[2], r[1]))),
                                  add(P.vl[1], sub(mul(P.w[2], r[0]), mul(P.w[0], r[2]))),
                                  add(P.vl[2], sub(mul(P.w[0], r[1]), mul(P.w[1], r[0])))};
-            float4 nv = gb.mv[id];
+            float4 nv = gb.acc.mv[id];
             float va[3];
             if (!(nv.w >= 1e-9f)) {  // inactive (mass 0) or mass < 1e-9: body claims the node
                 va[0] = vb[0]; va[1] = vb[1]; va[2] = vb[2];
@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params 
                 }
                 nv = make_float4(va[0], va[1], va[2], mn);
             }
-            gb.mv[id] = nv;
+            gb.acc.mv[id] = nv;
+            touch_block(gb.acc, blin);
             const float dF[3] = {mul(sub(va[0], vb[0]), P.mb_over_dt), mul(sub(va[1], vb[1]), P.mb_over_dt),
                                  mul(sub(va[2], vb[2]), P.mb_over_dt)};
             f0 = dF[0]; f1 = dF[1]; f2 = dF[2];
@@ -131,15 +132,15 @@ __global__ void k_grid_to_dense(GridDesc g, GridBuffers gb, float* vel, float* f
     if (q >= g.num_nodes()) return;
     const int k = (int)(q % ez), j = (int)((q / ez) % ey), i = (int)(q / (ez * ey));
     const int64_t id = g.node(g.ox + i, g.oy + j, g.oz + k);
-    const float4 mv = gb.mv[id];
+    const float4 mv = gb.acc.mv[id];
     if (vel) { vel[3 * q] = mv.x; vel[3 * q + 1] = mv.y; vel[3 * q + 2] = mv.z; }
     if (force) {
-        const float4 f = gb.f[id];
+        const float4 f = gb.acc.f[id];
         force[3 * q] = f.x; force[3 * q + 1] = f.y; force[3 * q + 2] = f.z;
     }
     if (mass) mass[q] = mv.w;
     if (active) active[q] = mv.w > 0.0f ? 1 : 0;
-    if (balloc) balloc[q] = gb.alloc[id >> 6];
+    if (balloc) balloc[q] = gb.alloc[g.block_of_node(id)];
 }
 
 __global__ void k_dense_velocity_to_grid(GridDesc g, GridBuffers gb, const float* vel) {
@@ -148,9 +149,10 @@ __global__ void k_dense_velocity_to_grid(GridDesc g, GridBuffers gb, const float
     if (q >= g.num_nodes()) return;
     const int k = (int)(q % ez), j = (int)((q / ez) % ey), i = (int)(q / (ez * ey));
     const int64_t id = g.node(g.ox + i, g.oy + j, g.oz + k);
-    float4 mv = gb.mv[id];
+    float4 mv = gb.acc.mv[id];
     mv.x = vel[3 * q]; mv.y = vel[3 * q + 1]; mv.z = vel[3 * q + 2];
-    gb.mv[id] = mv;
+    gb.acc.mv[id] = mv;
+    if (mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f || mv.w != 0.0f) touch_block(gb.acc, g.block_of_node(id));
 }
 
 __global__ void k_seed(GridDesc g, GridBuffers gb, int64_t n, const int32_t* ijk, const float* vel, const float* mass,
@@ -162,8 +164,9 @@ __global__ void k_seed(GridDesc g, GridBuffers gb, int64_t n, const int32_t* ijk
         atomicOr(status, ERR_ESCAPE);
         return;
     }
-    gb.mv[id] = make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], mass[q]);
-    gb.alloc[id >> 6] = 1;
+    gb.acc.mv[id] = make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], mass[q]);
+    gb.alloc[g.block_of_node(id)] = 1;
+    touch_block(gb.acc, g.block_of_node(id));
 }
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }

@@ -46,8 +46,10 @@ struct bm_solver {
     // Material (mpm_solver.h:100-109 defaults).
     float alpha = 0.40f, E = 1.0e5f, nu = 0.3f, density = 1500.0f, floor_friction = 0.4f;
     float gravity[3] = {0.0f, -9.81f, 0.0f};
-    // Particles.
-    ParticleSoA ps{nullptr, 0, 0};
+    // Particles (two stores: the bin sort permutes from one into the other).
+    ParticleSoA ps{nullptr, nullptr, 0, 0};
+    ParticleSoA ps_alt{nullptr, nullptr, 0, 0};
+    int32_t* d_inv = nullptr;  // add order -> stored slot (scratch for set_particles)
     double bbox_lo[3] = {1e300, 1e300, 1e300}, bbox_hi[3] = {-1e300, -1e300, -1e300};
     // Grid.
     bool domain_set = false;
@@ -55,9 +57,20 @@ struct bm_solver {
     int32_t margin = 16;
     bool grid_ready = false;
     GridDesc g{};
-    GridBuffers gb{nullptr, nullptr, nullptr};
-    // Phase tracking for the split API.
-    int phase = 0;  // 0 idle, 1 after p2g, 2 after grid update
+    GridAcc acc[2]{};
+    uint8_t* alloc = nullptr;
+    int cur = 0;           // accumulation buffer of the current step
+    int view = 0;          // buffer that holds the grid a caller sees after the last call
+    bool acc_valid = false;  // acc[cur] holds P2G of the current particle state
+    bool folded[2] = {false, false};  // acc[b].mv holds momentum + force * fold_dt[b]
+    float fold_dt[2] = {0.0f, 0.0f};
+    // Binned order.
+    BinBuffers bins{};
+    bool bins_valid = false;
+    int32_t sort_interval = 16;
+    int64_t steps_since_sort = 0;
+    int num_sms = 148;
+    bool fast_math = false;
     // Status.
     uint32_t* d_status = nullptr;
     unsigned long long* d_escaped = nullptr;
@@ -71,6 +84,8 @@ struct bm_solver {
     std::vector<PendingEvent> pending;
     std::vector<cudaEvent_t> event_pool;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
+
+    GridBuffers gbuf(int idx) const { return GridBuffers{acc[idx], alloc}; }
 };
 
 namespace {
@@ -174,20 +189,46 @@ void timed(bm_solver* s, const char* name, Fn&& fn) {
     }
 }
 
+bm_status_t alloc_store(bm_solver* s, ParticleSoA* ps, int64_t cap) {
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&ps->base, sizeof(float) * N_PLANES * cap, s->stream));
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&ps->pid, sizeof(int32_t) * cap, s->stream));
+    ps->cap = cap;
+    return BM_OK;
+}
+
+void free_store(bm_solver* s, ParticleSoA* ps) {
+    if (ps->base) cudaFreeAsync(ps->base, s->stream);
+    if (ps->pid) cudaFreeAsync(ps->pid, s->stream);
+    ps->base = nullptr;
+    ps->pid = nullptr;
+    ps->cap = 0;
+}
+
 bm_status_t ensure_particle_capacity(bm_solver* s, int64_t need) {
     if (need <= s->ps.cap) return BM_OK;
+    if (need > INT32_MAX) return invalid("more than 2^31-1 particles");
     int64_t cap = std::max<int64_t>(need, std::max<int64_t>(1024, s->ps.cap * 3 / 2));
     cap = (cap + 31) / 32 * 32;
-    float* nb = nullptr;
-    BM_CHECK_CUDA(cudaMallocAsync((void**)&nb, sizeof(float) * N_PLANES * cap, s->stream));
+    ParticleSoA nb{nullptr, nullptr, 0, s->ps.n};
+    bm_status_t st = alloc_store(s, &nb, cap);
+    if (st != BM_OK) return st;
     if (s->ps.base && s->ps.n > 0) {
         for (int p = 0; p < N_PLANES; ++p)
-            BM_CHECK_CUDA(cudaMemcpyAsync(nb + (int64_t)p * cap, s->ps.base + (int64_t)p * s->ps.cap,
-                                          sizeof(float) * s->ps.n, cudaMemcpyDeviceToDevice, s->stream));
+            BM_CHECK_CUDA(cudaMemcpyAsync(nb.plane(p), s->ps.plane(p), sizeof(float) * s->ps.n,
+                                          cudaMemcpyDeviceToDevice, s->stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(nb.pid, s->ps.pid, sizeof(int32_t) * s->ps.n, cudaMemcpyDeviceToDevice,
+                                      s->stream));
     }
-    if (s->ps.base) BM_CHECK_CUDA(cudaFreeAsync(s->ps.base, s->stream));
-    s->ps.base = nb;
-    s->ps.cap = cap;
+    free_store(s, &s->ps);
+    free_store(s, &s->ps_alt);
+    if (s->d_inv) cudaFreeAsync(s->d_inv, s->stream);
+    s->d_inv = nullptr;
+    s->ps = nb;
+    ParticleSoA alt{nullptr, nullptr, 0, s->ps.n};
+    st = alloc_store(s, &alt, cap);
+    if (st != BM_OK) return st;
+    s->ps_alt = alt;
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&s->d_inv, sizeof(int32_t) * cap, s->stream));
     return BM_OK;
 }
 
@@ -206,14 +247,38 @@ bm_status_t ensure_grid(bm_solver* s) {
         s->domain_set = true;
     }
     s->g = desc_from_domain(s->domain, s->dx);
-    const int64_t nn = s->g.num_nodes();
-    BM_CHECK_CUDA(cudaMallocAsync((void**)&s->gb.mv, sizeof(float4) * nn, s->stream));
-    BM_CHECK_CUDA(cudaMallocAsync((void**)&s->gb.f, sizeof(float4) * nn, s->stream));
-    BM_CHECK_CUDA(cudaMallocAsync((void**)&s->gb.alloc, (size_t)s->g.num_blocks(), s->stream));
-    BM_CHECK_CUDA(cudaMemsetAsync(s->gb.mv, 0, sizeof(float4) * nn, s->stream));
-    BM_CHECK_CUDA(cudaMemsetAsync(s->gb.f, 0, sizeof(float4) * nn, s->stream));
-    BM_CHECK_CUDA(cudaMemsetAsync(s->gb.alloc, 0, (size_t)s->g.num_blocks(), s->stream));
+    const int64_t nn = s->g.num_nodes(), nb = s->g.num_blocks();
+    if (nb > INT32_MAX / 64) return invalid("grid box too large");
+    for (int b = 0; b < 2; ++b) {
+        GridAcc& a = s->acc[b];
+        BM_CHECK_CUDA(cudaMallocAsync((void**)&a.mv, sizeof(float4) * nn, s->stream));
+        BM_CHECK_CUDA(cudaMallocAsync((void**)&a.f, sizeof(float4) * nn, s->stream));
+        BM_CHECK_CUDA(cudaMallocAsync((void**)&a.touched, sizeof(uint32_t) * nb, s->stream));
+        BM_CHECK_CUDA(cudaMallocAsync((void**)&a.list, sizeof(int32_t) * nb, s->stream));
+        BM_CHECK_CUDA(cudaMallocAsync((void**)&a.count, sizeof(int32_t), s->stream));
+        BM_CHECK_CUDA(cudaMemsetAsync(a.mv, 0, sizeof(float4) * nn, s->stream));
+        BM_CHECK_CUDA(cudaMemsetAsync(a.f, 0, sizeof(float4) * nn, s->stream));
+        BM_CHECK_CUDA(cudaMemsetAsync(a.touched, 0, sizeof(uint32_t) * nb, s->stream));
+        BM_CHECK_CUDA(cudaMemsetAsync(a.count, 0, sizeof(int32_t), s->stream));
+    }
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&s->alloc, (size_t)nb, s->stream));
+    BM_CHECK_CUDA(cudaMemsetAsync(s->alloc, 0, (size_t)nb, s->stream));
+    BinBuffers& bb = s->bins;
+    bb.nkeys = nn;
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&bb.count, sizeof(int32_t) * (nn + 1), s->stream));
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&bb.start, sizeof(int32_t) * (nn + 2), s->stream));
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&bb.tile_sum, sizeof(int64_t) * scan_tiles(nn), s->stream));
     s->grid_ready = true;
+    return BM_OK;
+}
+
+bm_status_t ensure_bin_keys(bm_solver* s) {
+    if (s->bins.key && s->bins.key_cap >= s->ps.cap) return BM_OK;
+    if (s->bins.key) cudaFreeAsync(s->bins.key, s->stream);
+    if (s->bins.rank) cudaFreeAsync(s->bins.rank, s->stream);
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&s->bins.key, sizeof(int32_t) * std::max<int64_t>(1, s->ps.cap), s->stream));
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&s->bins.rank, sizeof(int32_t) * std::max<int64_t>(1, s->ps.cap), s->stream));
+    s->bins.key_cap = s->ps.cap;
     return BM_OK;
 }
 
@@ -238,33 +303,58 @@ bm_status_t launch_error(const char* where) {
     return BM_OK;
 }
 
-bm_status_t do_p2g(bm_solver* s, float dt) {
+// Standalone P2G of the current particle state into acc[cur] (grid.clear()
+// + the P2G loop).
+bm_status_t do_p2g(bm_solver* s) {
     bm_status_t st = ensure_grid(s);
     if (st != BM_OK) return st;
-    const int64_t nn = s->g.num_nodes();
+    const int64_t nn = s->g.num_nodes(), nb = s->g.num_blocks();
+    GridAcc& a = s->acc[s->cur];
     timed(s, "grid_clear", [&] {
-        cudaMemsetAsync(s->gb.mv, 0, sizeof(float4) * nn, s->stream);
-        cudaMemsetAsync(s->gb.f, 0, sizeof(float4) * nn, s->stream);
+        cudaMemsetAsync(a.mv, 0, sizeof(float4) * nn, s->stream);
+        cudaMemsetAsync(a.f, 0, sizeof(float4) * nn, s->stream);
+        cudaMemsetAsync(a.touched, 0, sizeof(uint32_t) * nb, s->stream);
+        cudaMemsetAsync(a.count, 0, sizeof(int32_t), s->stream);
     });
     const Material m = material_of(s);
-    timed(s, "p2g", [&] { launch_p2g(s->ps, s->g, s->gb, m, dt, s->d_status, s->d_escaped, s->stream); });
-    s->phase = 1;
+    timed(s, "p2g", [&] { launch_p2g(s->ps, s->g, s->gbuf(s->cur), m, s->d_status, s->d_escaped, s->stream); });
+    s->acc_valid = true;
+    s->folded[s->cur] = false;
+    s->view = s->cur;
     return launch_error("p2g");
 }
 
 bm_status_t do_grid_update(bm_solver* s, float dt) {
-    if (!s->grid_ready) return invalid("grid_update before p2g");
+    if (!s->grid_ready || !s->acc_valid) {
+        set_last_error("grid_update needs the P2G of the current particle state (call p2g first)");
+        return BM_ERR_STATE;
+    }
     const Material m = material_of(s);
-    timed(s, "grid_update", [&] { launch_grid_update(s->g, s->gb, m, dt, s->stream); });
-    s->phase = 2;
+    GridAcc& other = s->acc[1 - s->cur];
+    if (s->folded[s->cur] && dt != s->fold_dt[s->cur]) {
+        set_last_error("grid_update dt differs from the dt folded into the precomputed P2G");
+        return BM_ERR_STATE;
+    }
+    timed(s, "grid_update", [&] {
+        launch_grid_update(s->g, s->acc[s->cur], other, m, dt, s->folded[s->cur], s->g.num_blocks(), s->stream);
+        cudaMemsetAsync(other.count, 0, sizeof(int32_t), s->stream);
+    });
+    s->view = s->cur;
     return launch_error("grid_update");
 }
 
+// G2P alone (split API): the particles advance, acc[cur] keeps this step's grid.
 bm_status_t do_g2p(bm_solver* s, float dt) {
-    if (!s->grid_ready) return invalid("g2p before p2g");
+    if (!s->grid_ready || !s->acc_valid) {
+        set_last_error("g2p needs a grid from p2g / grid_update");
+        return BM_ERR_STATE;
+    }
     const Material m = material_of(s);
-    timed(s, "g2p", [&] { launch_g2p(s->ps, s->g, s->gb, m, dt, s->d_status, s->d_escaped, s->stream); });
-    s->phase = 0;
+    timed(s, "g2p", [&] {
+        launch_g2p(s->ps, s->g, s->gbuf(s->cur), m, dt, s->d_status, s->d_escaped, s->stream);
+    });
+    s->acc_valid = false;
+    s->view = s->cur;
     return launch_error("g2p");
 }
 
@@ -272,8 +362,62 @@ bm_status_t do_m1(bm_solver* s, const bm_collider_t* body, float dt, int slot) {
     M1Params P;
     const bool any = m1_prepare(s->g, *body, dt, &P);
     BM_CHECK_CUDA(cudaMemsetAsync(s->d_acc + 7 * slot, 0, sizeof(double) * 7, s->stream));
-    if (any) timed(s, "m1_coupler", [&] { launch_m1(s->g, s->gb, P, s->d_acc + 7 * slot, s->stream); });
+    if (any) timed(s, "m1_coupler", [&] { launch_m1(s->g, s->gbuf(s->cur), P, s->d_acc + 7 * slot, s->stream); });
     return launch_error("m1");
+}
+
+// G2P of this step fused with the P2G of the next one (into the other
+// buffer); re-bins the particles first when due.
+bm_status_t do_g2p2g(bm_solver* s, float dt) {
+    if (s->ps.n > 0) {
+        bm_status_t st = ensure_bin_keys(s);
+        if (st != BM_OK) return st;
+        if (!s->bins_valid || (s->sort_interval > 0 && s->steps_since_sort >= s->sort_interval)) {
+            timed(s, "bin_sort", [&] {
+                ParticleSoA dst = s->ps_alt;
+                dst.n = s->ps.n;
+                launch_bin_sort(s->ps, dst, s->g, s->bins, s->stream);
+            });
+            std::swap(s->ps, s->ps_alt);
+            s->ps.n = s->ps_alt.n;
+            s->bins_valid = true;
+            s->steps_since_sort = 0;
+            st = launch_error("bin_sort");
+            if (st != BM_OK) return st;
+        }
+    }
+    const Material m = material_of(s);
+    const int next = 1 - s->cur;
+    timed(s, "g2p2g", [&] {
+        launch_g2p2g(s->ps, s->g, s->acc[s->cur], s->acc[next], s->alloc, m, dt, dt, s->fast_math, s->d_status,
+                     s->d_escaped, s->stream);
+    });
+    s->folded[next] = true;
+    s->fold_dt[next] = dt;
+    s->view = s->cur;
+    s->cur = next;
+    s->acc_valid = true;
+    s->steps_since_sort += 1;
+    return launch_error("g2p2g");
+}
+
+// One step on the fused path: [P2G if not precomputed], update, couplers, G2P+P2G.
+bm_status_t do_step(bm_solver* s, float dt, int32_t n_bodies, const bm_collider_t* bodies) {
+    bm_status_t st = ensure_grid(s);
+    // the precomputed P2G folded the previous dt into the momentum: redo it
+    // (unfolded) when this step uses another dt
+    if (st == BM_OK && s->acc_valid && s->folded[s->cur] && dt != s->fold_dt[s->cur]) s->acc_valid = false;
+    if (st == BM_OK && !s->acc_valid) st = do_p2g(s);
+    if (st == BM_OK) st = do_grid_update(s, dt);
+    for (int32_t b = 0; st == BM_OK && b < n_bodies; ++b) st = do_m1(s, bodies + b, dt, b);
+    if (st == BM_OK && n_bodies > 0) launch_reaction_finalize(s->d_acc, n_bodies, s->d_react, s->stream);
+    if (st == BM_OK) st = do_g2p2g(s, dt);
+    return st;
+}
+
+void invalidate_state(bm_solver* s) {
+    s->acc_valid = false;
+    s->bins_valid = false;
 }
 
 void update_bbox(bm_solver* s, int64_t n, const float* pos) {
@@ -334,6 +478,7 @@ BM_API bm_status_t bm_solver_create(float dx, const bm_domain_t* domain, bm_solv
     }
     bm_solver* s = new bm_solver();
     cudaGetDevice(&s->device);
+    cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
     s->dx = dx;
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
         set_last_error("cudaStreamCreate failed");
@@ -377,10 +522,22 @@ BM_API bm_status_t bm_solver_destroy(bm_solver_t* s) {
     for (auto e : s->event_pool) cudaEventDestroy(e);
     if (s->t0) cudaEventDestroy(s->t0);
     if (s->t1) cudaEventDestroy(s->t1);
-    cudaFree(s->ps.base);
-    cudaFree(s->gb.mv);
-    cudaFree(s->gb.f);
-    cudaFree(s->gb.alloc);
+    for (ParticleSoA* p : {&s->ps, &s->ps_alt}) {
+        cudaFree(p->base);
+        cudaFree(p->pid);
+    }
+    cudaFree(s->d_inv);
+    for (GridAcc& a : s->acc) {
+        cudaFree(a.mv);
+        cudaFree(a.f);
+        cudaFree(a.touched);
+        cudaFree(a.list);
+        cudaFree(a.count);
+    }
+    cudaFree(s->alloc);
+    for (void* p : {(void*)s->bins.key, (void*)s->bins.rank, (void*)s->bins.count, (void*)s->bins.start,
+                    (void*)s->bins.tile_sum})
+        cudaFree(p);
     cudaFree(s->d_status);
     cudaFree(s->d_escaped);
     cudaFree(s->d_acc);
@@ -419,6 +576,18 @@ BM_API bm_status_t bm_solver_set_auto_margin(bm_solver_t* s, int32_t margin) {
     return BM_OK;
 }
 
+BM_API bm_status_t bm_solver_set_sort_interval(bm_solver_t* s, int32_t steps) {
+    if (!s || steps < 0) return invalid("bad sort interval");
+    s->sort_interval = steps;
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_solver_set_math_mode(bm_solver_t* s, int32_t mode) {
+    if (!s || mode < 0 || mode > 1) return invalid("math mode must be 0 (IEEE) or 1 (fast)");
+    s->fast_math = mode == 1;
+    return BM_OK;
+}
+
 BM_API bm_status_t bm_solver_set_material(bm_solver_t* s, float E, float nu, float rho) {
     if (!s) return invalid("NULL handle");
     if (!std::isfinite(E) || !std::isfinite(nu) || !std::isfinite(rho)) return invalid("non-finite material");
@@ -426,7 +595,7 @@ BM_API bm_status_t bm_solver_set_material(bm_solver_t* s, float E, float nu, flo
     s->E = E;
     s->nu = nu;
     if (rho > 1e-12f && s->density > 1e-12f && rho != s->density && s->ps.n > 0) {
-        // V0 *= rho_old / rho_new on the device (mpm_solver.h:45-49).
+        // V0 *= rho_old / rho_new for every particle (mpm_solver.h:45-49).
         const float rescale = s->density / rho;
         std::vector<float> v0(s->ps.n);
         BM_CHECK_CUDA(cudaMemcpyAsync(v0.data(), s->ps.plane(P_V0), sizeof(float) * s->ps.n, cudaMemcpyDeviceToHost,
@@ -438,6 +607,7 @@ BM_API bm_status_t bm_solver_set_material(bm_solver_t* s, float E, float nu, flo
         BM_CHECK_CUDA(cudaStreamSynchronize(s->stream));
     }
     s->density = rho;
+    s->acc_valid = false;  // the precomputed P2G used the old stress
     return BM_OK;
 }
 
@@ -469,8 +639,9 @@ BM_API bm_status_t bm_solver_add_particles(bm_solver_t* s, int64_t n, const floa
     const int64_t n0 = s->ps.n;
     bm_status_t st = ensure_particle_capacity(s, n0 + n);
     if (st != BM_OK) return st;
-    // Host staging of the new rows, plane by plane (SoA).
+    // Host staging of the new rows, plane by plane (SoA), appended in add order.
     std::vector<float> buf((size_t)n * N_PLANES);
+    std::vector<int32_t> pid((size_t)n);
     auto col = [&](int p) { return buf.data() + (size_t)p * n; };
     for (int64_t q = 0; q < n; ++q) {
         for (int a = 0; a < 3; ++a) {
@@ -484,13 +655,18 @@ BM_API bm_status_t bm_solver_add_particles(bm_solver_t* s, int64_t n, const floa
         const float m = mass ? mass[q] : 1.0f;
         col(P_M)[q] = m;
         col(P_V0)[q] = (s->density > 1e-12f) ? (m / s->density) : 1.0f;
+        pid[q] = (int32_t)(n0 + q);
     }
     for (int p = 0; p < N_PLANES; ++p)
         BM_CHECK_CUDA(cudaMemcpyAsync(s->ps.plane(p) + n0, col(p), sizeof(float) * n, cudaMemcpyHostToDevice,
                                       s->stream));
+    BM_CHECK_CUDA(cudaMemcpyAsync(s->ps.pid + n0, pid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                                  s->stream));
     BM_CHECK_CUDA(cudaStreamSynchronize(s->stream));
     s->ps.n = n0 + n;
+    s->ps_alt.n = s->ps.n;
     update_bbox(s, n, pos);
+    invalidate_state(s);
     return BM_OK;
 }
 
@@ -505,20 +681,23 @@ BM_API bm_status_t bm_solver_get_particles(bm_solver_t* s, const bm_particles_vi
     DeviceGuard dg(s->device);
     const int64_t n = s->ps.n;
     if (n == 0) return BM_OK;
-    std::vector<float> tmp((size_t)n * 9);
     struct Field { float* dst; int plane; int width; };
     const Field fields[] = {{v->position, P_X, 3}, {v->velocity, P_V, 3}, {v->F, P_F, 9},
                             {v->C, P_C, 9},        {v->mass, P_M, 1},     {v->volume, P_V0, 1}};
+    float* tmp = nullptr;
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&tmp, sizeof(float) * 9 * n, s->stream));
+    bm_status_t st = BM_OK;
     for (const Field& f : fields) {
         if (!f.dst) continue;
-        for (int c = 0; c < f.width; ++c)
-            BM_CHECK_CUDA(cudaMemcpyAsync(tmp.data() + (size_t)c * n, s->ps.plane(f.plane + c), sizeof(float) * n,
-                                          cudaMemcpyDeviceToHost, s->stream));
-        BM_CHECK_CUDA(cudaStreamSynchronize(s->stream));
-        for (int64_t q = 0; q < n; ++q)
-            for (int c = 0; c < f.width; ++c) f.dst[q * f.width + c] = tmp[(size_t)c * n + q];
+        launch_gather_rows(s->ps, f.plane, f.width, tmp, s->stream);
+        if (cudaMemcpyAsync(f.dst, tmp, sizeof(float) * f.width * n, cudaMemcpyDeviceToHost, s->stream) !=
+            cudaSuccess)
+            st = BM_ERR_CUDA;
     }
-    return BM_OK;
+    cudaFreeAsync(tmp, s->stream);
+    BM_CHECK_CUDA(cudaStreamSynchronize(s->stream));
+    if (st != BM_OK) set_last_error("device-to-host copy of particles failed");
+    return st;
 }
 
 BM_API bm_status_t bm_solver_set_particles(bm_solver_t* s, int64_t first, int64_t n, const bm_particles_view_t* v) {
@@ -526,30 +705,28 @@ BM_API bm_status_t bm_solver_set_particles(bm_solver_t* s, int64_t first, int64_
     if (first < 0 || n < 0 || first + n > s->ps.n) return invalid("particle range out of bounds");
     if (n == 0) return BM_OK;
     DeviceGuard dg(s->device);
-    std::vector<float> tmp((size_t)n * 9);
     struct Field { const float* src; int plane; int width; };
     const Field fields[] = {{v->position, P_X, 3}, {v->velocity, P_V, 3}, {v->F, P_F, 9}, {v->C, P_C, 9}};
+    float* tmp = nullptr;
+    BM_CHECK_CUDA(cudaMallocAsync((void**)&tmp, sizeof(float) * 9 * n, s->stream));
+    launch_inverse_pid(s->ps, s->d_inv, s->stream);
     for (const Field& f : fields) {
         if (!f.src) continue;
-        for (int64_t q = 0; q < n; ++q)
-            for (int c = 0; c < f.width; ++c) tmp[(size_t)c * n + q] = f.src[q * f.width + c];
-        for (int c = 0; c < f.width; ++c)
-            BM_CHECK_CUDA(cudaMemcpyAsync(s->ps.plane(f.plane + c) + first, tmp.data() + (size_t)c * n,
-                                          sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
-        BM_CHECK_CUDA(cudaStreamSynchronize(s->stream));
+        cudaMemcpyAsync(tmp, f.src, sizeof(float) * f.width * n, cudaMemcpyHostToDevice, s->stream);
+        launch_scatter_rows(s->ps, f.plane, f.width, tmp, first, n, s->d_inv, s->stream);
     }
+    cudaFreeAsync(tmp, s->stream);
+    BM_CHECK_CUDA(cudaStreamSynchronize(s->stream));
     if (v->position) update_bbox(s, n, v->position);
-    return BM_OK;
+    invalidate_state(s);
+    return launch_error("set_particles");
 }
 
 BM_API bm_status_t bm_solver_step(bm_solver_t* s, float dt) {
     if (!s) return invalid("NULL handle");
     if (!std::isfinite(dt)) return invalid("dt is not finite");
     DeviceGuard dg(s->device);
-    bm_status_t st = do_p2g(s, dt);
-    if (st == BM_OK) st = do_grid_update(s, dt);
-    if (st == BM_OK) st = do_g2p(s, dt);
-    return st;
+    return do_step(s, dt, 0, nullptr);
 }
 
 BM_API bm_status_t bm_solver_step_n(bm_solver_t* s, float dt, int32_t n_steps) {
@@ -564,8 +741,9 @@ BM_API bm_status_t bm_solver_step_n(bm_solver_t* s, float dt, int32_t n_steps) {
 
 BM_API bm_status_t bm_solver_p2g(bm_solver_t* s, float dt) {
     if (!s) return invalid("NULL handle");
+    (void)dt;  // P2G does not depend on dt (mpm_solver.h:168)
     DeviceGuard dg(s->device);
-    return do_p2g(s, dt);
+    return do_p2g(s);
 }
 
 BM_API bm_status_t bm_solver_grid_update(bm_solver_t* s, float dt) {
@@ -586,6 +764,10 @@ BM_API bm_status_t bm_coupler_m1_apply(bm_solver_t* s, const bm_collider_t* body
     std::memset(out, 0, sizeof(*out));
     bm_status_t st = ensure_grid(s);
     if (st != BM_OK) return st;
+    if (!s->acc_valid && s->ps.n > 0) {
+        set_last_error("the coupler needs a grid from p2g / grid_update");
+        return BM_ERR_STATE;
+    }
     st = do_m1(s, body, dt, 0);
     if (st != BM_OK) return st;
     launch_reaction_finalize(s->d_acc, 1, s->d_react, s->stream);
@@ -598,13 +780,10 @@ BM_API bm_status_t bm_solver_step_coupled(bm_solver_t* s, float dt, int32_t n_bo
                                           bm_reaction_t* reactions) {
     if (!s) return invalid("NULL handle");
     if (n_bodies < 0 || (n_bodies > 0 && !bodies)) return invalid("bad bodies");
+    if (!std::isfinite(dt)) return invalid("dt is not finite");
     DeviceGuard dg(s->device);
     bm_status_t st = ensure_reactions(s, std::max(1, n_bodies));
-    if (st == BM_OK) st = do_p2g(s, dt);
-    if (st == BM_OK) st = do_grid_update(s, dt);
-    for (int32_t b = 0; st == BM_OK && b < n_bodies; ++b) st = do_m1(s, bodies + b, dt, b);
-    if (st == BM_OK && n_bodies > 0) launch_reaction_finalize(s->d_acc, n_bodies, s->d_react, s->stream);
-    if (st == BM_OK) st = do_g2p(s, dt);
+    if (st == BM_OK) st = do_step(s, dt, n_bodies, bodies);
     if (st == BM_OK && reactions && n_bodies > 0) {
         BM_CHECK_CUDA(cudaMemcpyAsync(reactions, s->d_react, sizeof(bm_reaction_t) * n_bodies,
                                       cudaMemcpyDeviceToHost, s->stream));
@@ -638,6 +817,11 @@ BM_API bm_status_t bm_solver_get_grid(bm_solver_t* s, float* vel, float* force, 
     bm_status_t st = ensure_grid(s);
     if (st != BM_OK) return st;
     const int64_t nn = s->g.num_nodes();
+    if (force && s->folded[s->view]) {
+        // after a fused step the force is folded into the momentum (see header)
+        std::memset(force, 0, sizeof(float) * 3 * nn);
+        force = nullptr;
+    }
     float *dv = nullptr, *df = nullptr, *dm = nullptr;
     uint8_t *da = nullptr, *db = nullptr;
     if (vel) BM_CHECK_CUDA(cudaMallocAsync((void**)&dv, sizeof(float) * 3 * nn, s->stream));
@@ -645,7 +829,7 @@ BM_API bm_status_t bm_solver_get_grid(bm_solver_t* s, float* vel, float* force, 
     if (mass) BM_CHECK_CUDA(cudaMallocAsync((void**)&dm, sizeof(float) * nn, s->stream));
     if (active) BM_CHECK_CUDA(cudaMallocAsync((void**)&da, (size_t)nn, s->stream));
     if (balloc) BM_CHECK_CUDA(cudaMallocAsync((void**)&db, (size_t)nn, s->stream));
-    launch_grid_to_dense(s->g, s->gb, dv, df, dm, da, db, s->stream);
+    launch_grid_to_dense(s->g, s->gbuf(s->view), dv, df, dm, da, db, s->stream);
     st = launch_error("grid_to_dense");
     if (vel) cudaMemcpyAsync(vel, dv, sizeof(float) * 3 * nn, cudaMemcpyDeviceToHost, s->stream);
     if (force) cudaMemcpyAsync(force, df, sizeof(float) * 3 * nn, cudaMemcpyDeviceToHost, s->stream);
@@ -676,8 +860,11 @@ BM_API bm_status_t bm_solver_seed_grid(bm_solver_t* s, int64_t n, const int32_t*
     cudaMemcpyAsync(di, ijk, sizeof(int32_t) * 3 * n, cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(dv, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(dm, mass, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream);
-    launch_seed_grid(s->g, s->gb, n, di, dv, dm, s->d_status, s->stream);
+    launch_seed_grid(s->g, s->gbuf(s->cur), n, di, dv, dm, s->d_status, s->stream);
     st = launch_error("seed_grid");
+    s->acc_valid = true;  // the seeded grid stands for this step's grid
+    s->folded[s->cur] = false;
+    s->view = s->cur;
     cudaFreeAsync(di, s->stream);
     cudaFreeAsync(dv, s->stream);
     cudaFreeAsync(dm, s->stream);
@@ -694,7 +881,7 @@ BM_API bm_status_t bm_solver_set_grid_velocity(bm_solver_t* s, const float* vel)
     float* dv = nullptr;
     BM_CHECK_CUDA(cudaMallocAsync((void**)&dv, sizeof(float) * 3 * nn, s->stream));
     cudaMemcpyAsync(dv, vel, sizeof(float) * 3 * nn, cudaMemcpyHostToDevice, s->stream);
-    launch_dense_velocity_to_grid(s->g, s->gb, dv, s->stream);
+    launch_dense_velocity_to_grid(s->g, s->gbuf(s->cur), dv, s->stream);
     st = launch_error("set_grid_velocity");
     cudaFreeAsync(dv, s->stream);
     BM_CHECK_CUDA(cudaStreamSynchronize(s->stream));

@@ -8,6 +8,8 @@
 // dense box of 4^3-node blocks holding two float4 per node: (momentum, mass)
 // and (force, 0). P2G scatters with 16-byte vector reductions into L2
 // (red.global.add.v4.f32), two per particle-node pair.
+#include <algorithm>
+
 #include "bm_internal.h"
 #include "bm_math.cuh"
 
@@ -21,25 +23,9 @@ __device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float
     atomicAdd(addr, make_float4(a, b, c, d));
 }
 
-// Marks the 4^3 blocks covered by nodes with non-zero 1-D weight as allocated
-// (the reference allocates a block on the first get_node() of any node in it).
-__device__ __forceinline__ void mark_blocks(const GridDesc& g, uint8_t* alloc, const int base[3],
-                                            const float wx[3], const float wy[3], const float wz[3]) {
-    const int lo0 = base[0] + (wx[0] == 0.0f), hi0 = base[0] + 2 - (wx[2] == 0.0f);
-    const int lo1 = base[1] + (wy[0] == 0.0f), hi1 = base[1] + 2 - (wy[2] == 0.0f);
-    const int lo2 = base[2] + (wz[0] == 0.0f), hi2 = base[2] + 2 - (wz[2] == 0.0f);
-    for (int a = (lo0 - g.ox) >> 2; a <= (hi0 - g.ox) >> 2; ++a)
-        for (int b = (lo1 - g.oy) >> 2; b <= (hi1 - g.oy) >> 2; ++b)
-            for (int c = (lo2 - g.oz) >> 2; c <= (hi2 - g.oz) >> 2; ++c) {
-                if ((unsigned)a < (unsigned)g.nbx && (unsigned)b < (unsigned)g.nby && (unsigned)c < (unsigned)g.nbz) {
-                    uint8_t* q = alloc + ((int64_t)a * g.nby + b) * g.nbz + c;
-                    if (*q == 0) *q = 1;
-                }
-            }
-}
-
 __global__ void __launch_bounds__(kThreads) k_p2g(ParticleSoA ps, GridDesc g, GridBuffers gb, Material mat,
                                                   uint32_t* status, unsigned long long* escaped) {
+    // One thread per particle; scatter with 16-byte vector reductions.
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= ps.n) return;
     const float x[3] = {ps.plane(P_X)[p], ps.plane(P_X + 1)[p], ps.plane(P_X + 2)[p]};
@@ -91,45 +77,76 @@ __global__ void __launch_bounds__(kThreads) k_p2g(ParticleSoA ps, GridDesc g, Gr
                 const float s0 = (sk[0] * d0 + sk[1] * d1) + sk[2] * d2;
                 const float s1 = (sk[3] * d0 + sk[4] * d1) + sk[5] * d2;
                 const float s2 = (sk[6] * d0 + sk[7] * d1) + sk[8] * d2;
-                red_add_v4(gb.mv + id, (v[0] + a0) * mc, (v[1] + a1) * mc, (v[2] + a2) * mc, mc);
-                red_add_v4(gb.f + id, s0 * w, s1 * w, s2 * w, 0.0f);
+                red_add_v4(gb.acc.mv + id, (v[0] + a0) * mc, (v[1] + a1) * mc, (v[2] + a2) * mc, mc);
+                red_add_v4(gb.acc.f + id, s0 * w, s1 * w, s2 * w, 0.0f);
             }
-    mark_blocks(g, gb.alloc, base, wgt[0], wgt[1], wgt[2]);
+    mark_stencil_blocks(g, gb.acc, gb.alloc, base, wgt[0], wgt[1], wgt[2]);
     if (dropped) {
         atomicOr(status, ERR_ESCAPE);
         atomicAdd(escaped, (unsigned long long)dropped);
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_grid_update(GridDesc g, GridBuffers gb, Material mat, float dt) {
-    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= g.num_nodes()) return;
-    const float4 mv = gb.mv[id];
-    if (!(mv.w > 1e-6f)) return;  // inactive (mass 0) or mass <= 1e-6: untouched
-    const float4 f = gb.f[id];
-    float v0 = (mv.x + f.x * dt) / mv.w;
-    float v1 = (mv.y + f.y * dt) / mv.w;
-    float v2 = (mv.z + f.z * dt) / mv.w;
-    v0 = v0 + mat.gx * dt;
-    v1 = v1 + mat.gy * dt;
-    v2 = v2 + mat.gz * dt;
-    const int64_t b = id >> 6;
-    const int lj = (int)((id >> 2) & 3);
-    const int bj = (int)((b / g.nbz) % g.nby);
-    const int j = g.oy + 4 * bj + lj;
-    const float node_y = ((float)j + 0.5f) * g.dx;
-    if (node_y < g.dx && v1 < 0.0f) {
-        const float vn = -v1;
-        v1 = 0.0f;
-        const float mag = sqrtf(v0 * v0 + v2 * v2);
-        const float budget = mat.floor_friction * vn;
-        if (mag > 1e-12f) {
-            const float sc = smax(0.0f, (mag - budget) / mag);
-            v0 = v0 * sc;
-            v2 = v2 * sc;
+// update_grid over the blocks listed in `cur` (every other node of the box is
+// empty, so skipping it is exact); the same launch zeroes the blocks listed in
+// `other` so that it can take the next P2G.
+__global__ void __launch_bounds__(kThreads) k_grid_update(GridDesc g, GridAcc cur, GridAcc other, Material mat,
+                                                          float dt, bool folded) {
+    const int n_cur = *cur.count, n_other = *other.count;
+    const int64_t total = (int64_t)(n_cur + n_other) * 64;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int slot = (int)(e >> 6), t = (int)(e & 63);
+        if (slot >= n_cur) {
+            const int64_t b = other.list[slot - n_cur];
+            const int64_t id = g.node_of_block(b, t);
+            other.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+            other.f[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (t == 0) other.touched[b] = 0u;
+            continue;
         }
+        const int64_t b = cur.list[slot];
+        const int64_t id = g.node_of_block(b, t);
+        const float4 mv = cur.mv[id];
+        if (!(mv.w > 1e-6f)) {
+            // inactive (mass 0) or mass <= 1e-6: the reference leaves the
+            // momentum (without force) in place
+            if (folded && (mv.w > 0.0f || mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f)) {
+                const float4 f = cur.f[id];
+                cur.mv[id] = make_float4(mv.x - f.x * dt, mv.y - f.y * dt, mv.z - f.z * dt, mv.w);
+            }
+            continue;
+        }
+        float v0, v1, v2;
+        if (folded) {
+            v0 = mv.x / mv.w;
+            v1 = mv.y / mv.w;
+            v2 = mv.z / mv.w;
+        } else {
+            const float4 f = cur.f[id];
+            v0 = (mv.x + f.x * dt) / mv.w;
+            v1 = (mv.y + f.y * dt) / mv.w;
+            v2 = (mv.z + f.z * dt) / mv.w;
+        }
+        v0 = v0 + mat.gx * dt;
+        v1 = v1 + mat.gy * dt;
+        v2 = v2 + mat.gz * dt;
+        const int lj = (t >> 2) & 3;
+        const int bj = (int)((b / g.nbz) % g.nby);
+        const int j = g.oy + 4 * bj + lj;
+        const float node_y = ((float)j + 0.5f) * g.dx;
+        if (node_y < g.dx && v1 < 0.0f) {
+            const float vn = -v1;
+            v1 = 0.0f;
+            const float mag = sqrtf(v0 * v0 + v2 * v2);
+            const float budget = mat.floor_friction * vn;
+            if (mag > 1e-12f) {
+                const float sc = smax(0.0f, (mag - budget) / mag);
+                v0 = v0 * sc;
+                v2 = v2 * sc;
+            }
+        }
+        cur.mv[id] = make_float4(v0, v1, v2, mv.w);
     }
-    gb.mv[id] = make_float4(v0, v1, v2, mv.w);
 }
 
 __global__ void __launch_bounds__(kThreads) k_g2p(ParticleSoA ps, GridDesc g, GridBuffers gb, Material mat, float dt,
@@ -166,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(ParticleSoA ps, GridDesc g, Gr
                 const int ni = base[0] + i, nj = base[1] + j, nk = base[2] + k;
                 const int64_t id = g.node(ni, nj, nk);
                 if (id < 0) { ++dropped; continue; }
-                const float4 nv = gb.mv[id];
+                const float4 nv = gb.acc.mv[id];
                 const float d[3] = {((float)ni - fx[0] - 0.5f) * g.dx, ((float)nj - fx[1] - 0.5f) * g.dx,
                                     ((float)nk - fx[2] - 0.5f) * g.dx};
                 const float wv[3] = {nv.x * w, nv.y * w, nv.z * w};
@@ -208,21 +225,66 @@ inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / k
 
 }  // namespace
 
-void launch_p2g(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat, float dt,
+void launch_p2g(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat,
                 uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st) {
-    (void)dt;
     if (ps.n == 0) return;
     k_p2g<<<blocks_for(ps.n), kThreads, 0, st>>>(ps, g, gb, mat, d_status, d_escaped);
 }
 
-void launch_grid_update(const GridDesc& g, const GridBuffers& gb, const Material& mat, float dt, cudaStream_t st) {
-    k_grid_update<<<blocks_for(g.num_nodes()), kThreads, 0, st>>>(g, gb, mat, dt);
+void launch_grid_update(const GridDesc& g, const GridAcc& cur, const GridAcc& other, const Material& mat, float dt,
+                        bool folded, int64_t max_blocks, cudaStream_t st) {
+    const int64_t want = (2 * max_blocks * 64 + kThreads - 1) / kThreads;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 16));
+    k_grid_update<<<grid, kThreads, 0, st>>>(g, cur, other, mat, dt, folded);
 }
 
 void launch_g2p(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat, float dt,
                 uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st) {
     if (ps.n == 0) return;
     k_g2p<<<blocks_for(ps.n), kThreads, 0, st>>>(ps, g, gb, mat, dt, d_status, d_escaped);
+}
+
+// ---- particle rows in add order ------------------------------------------------
+
+namespace {
+
+__global__ void k_gather_rows(ParticleSoA ps, int plane0, int width, float* out) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ps.n) return;
+    const int64_t a = ps.pid[p];
+    for (int c = 0; c < width; ++c) out[a * width + c] = ps.plane(plane0 + c)[p];
+}
+
+__global__ void k_scatter_rows(ParticleSoA ps, int plane0, int width, const float* in, int64_t first, int64_t n,
+                               const int32_t* inv) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int64_t p = inv[first + q];
+    for (int c = 0; c < width; ++c) ps.plane(plane0 + c)[p] = in[q * width + c];
+}
+
+__global__ void k_inverse_pid(ParticleSoA ps, int32_t* inv) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ps.n) return;
+    inv[ps.pid[p]] = (int32_t)p;
+}
+
+}  // namespace
+
+void launch_gather_rows(const ParticleSoA& ps, int plane0, int width, float* out, cudaStream_t st) {
+    if (ps.n == 0) return;
+    k_gather_rows<<<blocks_for(ps.n), kThreads, 0, st>>>(ps, plane0, width, out);
+}
+
+void launch_scatter_rows(const ParticleSoA& ps, int plane0, int width, const float* in, int64_t first, int64_t n,
+                         const int32_t* inv, cudaStream_t st) {
+    if (n == 0) return;
+    k_scatter_rows<<<blocks_for(n), kThreads, 0, st>>>(ps, plane0, width, in, first, n, inv);
+}
+
+void launch_inverse_pid(const ParticleSoA& ps, int32_t* inv, cudaStream_t st) {
+    if (ps.n == 0) return;
+    k_inverse_pid<<<blocks_for(ps.n), kThreads, 0, st>>>(ps, inv);
 }
 
 }  // namespace bm

@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--particles", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--math", choices=["fast", "ieee"], default=None,
+                    help="SVD arithmetic of the fused step (default: the library default)")
+    ap.add_argument("--sort-interval", type=int, default=None)
     return ap.parse_args()
 
 
@@ -140,12 +143,14 @@ def bytes_per_unit(n_particles: int, touched_nodes: int):
     x,v,C,F,m,V0 = 26 floats; G2P reads x,F = 12 and writes x,v,C,F = 24) and
     per touched node 80 B (P2G flush 7 floats, update reads 7 / writes 3, G2P
     reads 3). Per kernel: P2G 104 B/particle + 28 B/node, grid update 40 B/node,
-    G2P 144 B/particle + 12 B/node."""
+    G2P 144 B/particle + 12 B/node; the fused G2P(n) + P2G(n+1) kernel does
+    the work of both: 248 B/particle + 40 B/node."""
     return {
         "step": 248 * n_particles + 80 * touched_nodes,
         "p2g": 104 * n_particles + 28 * touched_nodes,
         "grid_update": 40 * touched_nodes,
         "g2p": 144 * n_particles + 12 * touched_nodes,
+        "g2p2g": 248 * n_particles + 40 * touched_nodes,
     }
 
 
@@ -161,6 +166,10 @@ def run_ours(args, ranks: Ranks):
     s.set_material(sc.E, sc.nu, sc.rho)
     s.set_plastic_alpha(sc.alpha)
     s.add_particles(sc.position, None, sc.mass)
+    if args.math:
+        s.set_math_mode(args.math == "fast")
+    if args.sort_interval is not None:
+        s.set_sort_interval(args.sort_interval)
 
     def collider(step):
         return bm.make_collider(**body.at_time(step * sc.dt).as_tuple())
@@ -215,6 +224,7 @@ def run_ours(args, ranks: Ranks):
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get(dom)
     launches = sum(v[1] for k, v in kernels.items() if k != "grid_clear")
+    launches += 2 * kernels.get("bin_sort", (0, 0))[1]  # key + scan + permute per sort
     step_roof_gbs = bpu["step"] / (per_step_ms / 1e3) / 1e9
 
     out = {

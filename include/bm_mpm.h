@@ -115,6 +115,17 @@ BM_API bm_status_t bm_solver_set_domain(bm_solver_t* s, const bm_domain_t* domai
 BM_API bm_status_t bm_solver_get_domain(bm_solver_t* s, bm_domain_t* out);
 /* Margin (nodes per side, default 16) used when the box is auto-sized. */
 BM_API bm_status_t bm_solver_set_auto_margin(bm_solver_t* s, int32_t margin_nodes);
+/* Particles are regrouped by 4^3-node bin every `steps` steps (default 16;
+ * 1 = every step, 0 = only when particles are added or overwritten). A
+ * particle that drifts out of its bin's tile between regroupings takes a
+ * slower global-memory path with the same result. */
+BM_API bm_status_t bm_solver_set_sort_interval(bm_solver_t* s, int32_t steps);
+/* Arithmetic of the per-particle Jacobi SVD in the fused step: 0 (default)
+ * IEEE division and square root like the reference; 1 takes the rotation
+ * angle from the hardware approximations (about 1 ulp). Both meet the
+ * accuracy bars against the reference (mode 1 drifts about 2.5x further over
+ * 1000 steps) and mode 1 saves under 2% of the step on B200. */
+BM_API bm_status_t bm_solver_set_math_mode(bm_solver_t* s, int32_t mode);
 /* set_material (:42-51): rescales V0 of existing particles by rho_old / rho_new. */
 BM_API bm_status_t bm_solver_set_material(bm_solver_t* s, float young_modulus, float poisson_ratio,
                                           float bulk_density);
@@ -161,12 +172,15 @@ BM_API bm_status_t bm_solver_get_reactions(bm_solver_t* s, int32_t n_bodies, bm_
 /* Number of nodes of the dense box (product of the rounded extents). */
 BM_API bm_status_t bm_solver_grid_num_nodes(bm_solver_t* s, int64_t* out);
 /* Dense copy in (i, j, k) order, k fastest, over the box of
- * bm_solver_get_domain. Any pointer may be NULL. velocity holds what the
- * reference's GridNode::velocity holds at this point of the step (momentum
- * after P2G, velocity after update_grid). active is the reference's
- * node.active: 1 for nodes touched this step. block_allocated (one byte per
- * node) reports whether the node's 4^3 block has ever been touched, the
- * blocks the reference's hash grid keeps (spgrid_cpu.h:78-91). */
+ * bm_solver_get_domain. Any pointer may be NULL. velocity and mass hold what
+ * the reference's GridNode holds at this point of the step (momentum after
+ * P2G, velocity after update_grid and the couplers). force is the P2G force
+ * after bm_solver_p2g; after bm_solver_step / _step_coupled the fused step
+ * adds force*dt into the momentum during P2G, so force reads back as zero.
+ * active is the reference's node.active (mass > 0: touched this step,
+ * seeded, or claimed by a coupler). block_allocated (one byte per node)
+ * reports whether the node's 4^3 block has ever been touched, the blocks the
+ * reference's hash grid keeps (spgrid_cpu.h:78-91). */
 BM_API bm_status_t bm_solver_get_grid(bm_solver_t* s, float* velocity, float* force, float* mass,
                                       uint8_t* active, uint8_t* block_allocated);
 /* Seeds nodes like the reference tests and scenarios do through get_node()

@@ -55,7 +55,11 @@ def test_small_scene_phases_match_reference_fixture():
     s.step(1e-4, 19)
     p = s.get_particles()
     assert max_err_dx(p["position"], d["pos20"], dx) < POS_TOL_100
-    np.testing.assert_allclose(p["F"], d["F20"], atol=1e-5)
+    # F of yielding particles carries the reference SVD's own error: its Jacobi
+    # stops at an absolute off-diagonal of 1e-5 (svd.h:83), so any change of
+    # rounding moves F at that order. The FP64 restatement differs from the
+    # FP32 reference by 7.1e-6 here; the bar is 3e-5.
+    np.testing.assert_allclose(p["F"], d["F20"], atol=3e-5)
     assert s.sync() == (0, 0)
 
 
@@ -69,9 +73,11 @@ def test_mass_conservation_after_p2g():
     assert abs(grid_mass - pm) / pm < MASS_REL_TOL
 
 
-def test_sand_column_100_and_1000_steps():
+@pytest.mark.parametrize("fast_math", [True, False], ids=["fast-svd", "ieee-svd"])
+def test_sand_column_100_and_1000_steps(fast_math):
     sc = scenes.sand_column()
     g, c = scene_solvers(sc, REF)
+    g.set_math_mode(fast_math)
     f64 = cpu_solver("f64", sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
     g.step(sc.dt, 100)
     c.step(sc.dt, 100)
@@ -194,3 +200,56 @@ def test_edge_cases():
         s.step(float("nan"))
     with pytest.raises(bm.BMError):
         s.set_particles(5, position=np.zeros((1, 3), np.float32))
+
+
+def test_bin_regrouping_interval_does_not_change_results():
+    """Regrouping every step, every 16 steps or never give the same particles
+    (up to FP32-atomic order) and all match the reference."""
+    sc = scenes.sand_column()
+    ref = cpu_solver(REF, sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+    ref.step(sc.dt, 60)
+    pr = ref.get_particles()["position"]
+    for interval in (1, 16, 0):
+        s = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+        s.set_sort_interval(interval)
+        s.step(sc.dt, 60)
+        assert max_err_dx(s.get_particles()["position"], pr, sc.dx) < POS_TOL_100, interval
+        assert s.sync() == (0, 0)
+
+
+def test_particles_leaving_their_tile_take_the_global_path():
+    """Fast particles never regrouped drift many cells away from their bin's
+    shared-memory tile; the global-memory path must give the reference result."""
+    rng = np.random.RandomState(5)
+    dx = 1.0 / 32
+    pos = (np.array([0.3, 0.2, 0.3]) + rng.random_sample((3000, 3)) * 0.2).astype(np.float32)
+    vel = np.tile(np.array([[6.0, 1.0, -4.0]], np.float32), (3000, 1))
+    vel += (rng.standard_normal((3000, 3)) * 0.1).astype(np.float32)
+    m = np.full(3000, 1600 * dx ** 3 / 8, np.float32)
+    kw = dict(E=3.5e5, nu=0.3, rho=1600.0, alpha=scenes.dp_alpha(30), gravity=(0, 0, 0))
+    g = gpu_solver(dx, pos, vel, m, margin=40, **kw)
+    g.set_sort_interval(0)
+    c = cpu_solver(REF, dx, pos, vel, m, **kw)
+    g.step(5e-4, 40)   # ~0.1 cell per step: 4 cells of drift without regrouping
+    c.step(5e-4, 40)
+    assert max_err_dx(g.get_particles()["position"], c.get_particles()["position"], dx) < POS_TOL_100
+    assert g.sync() == (0, 0)
+
+
+def test_get_and_set_particles_keep_add_order():
+    sc = scenes.sand_column()
+    s = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+    s.set_sort_interval(1)
+    s.step(sc.dt, 3)  # particles are now stored in bin order
+    p = s.get_particles()
+    F = p["F"].copy()
+    F[::97] = np.diag([1.0, 0.97, 1.0]).astype(np.float32)
+    s.set_particles(0, F=F)
+    q = s.get_particles()
+    assert np.array_equal(q["F"], F) and np.array_equal(q["position"], p["position"])
+    r = cpu_solver(REF, sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+    r.step(sc.dt, 3)
+    r.set_particle_state(0, F=F)
+    s.step(sc.dt, 10)
+    r.step(sc.dt, 10)
+    assert max_err_dx(s.get_particles()["position"], r.get_particles()["position"], sc.dx) < POS_TOL_100
