@@ -75,6 +75,9 @@ _SIGS = {
     "bm_solver_set_auto_margin": (_st, [_h, C.c_int32]),
     "bm_solver_set_sort_interval": (_st, [_h, C.c_int32]),
     "bm_solver_set_math_mode": (_st, [_h, C.c_int32]),
+    "bm_solver_set_launch_variant": (_st, [_h, C.c_int32]),
+    "bm_launch_variant_count": (C.c_int32, []),
+    "bm_launch_variant_name": (C.c_char_p, [C.c_int32]),
     "bm_solver_set_material": (_st, [_h, C.c_float, C.c_float, C.c_float]),
     "bm_solver_set_gravity": (_st, [_h, _f]),
     "bm_solver_set_plastic_alpha": (_st, [_h, C.c_float]),
@@ -126,6 +129,11 @@ def lib():
 
 def set_device(device: int):
     check(lib().bm_set_device(int(device)), "bm_set_device")
+
+
+def launch_variants():
+    L = lib()
+    return [L.bm_launch_variant_name(i).decode() for i in range(L.bm_launch_variant_count())]
 
 
 def declared_symbols():
@@ -197,6 +205,9 @@ class MPMSolver:
 
     def set_sort_interval(self, steps: int):
         check(lib().bm_solver_set_sort_interval(self._h, int(steps)), "bm_solver_set_sort_interval")
+
+    def set_launch_variant(self, variant: int):
+        check(lib().bm_solver_set_launch_variant(self._h, int(variant)), "bm_solver_set_launch_variant")
 
     def set_math_mode(self, fast: bool):
         check(lib().bm_solver_set_math_mode(self._h, 1 if fast else 0), "bm_solver_set_math_mode")

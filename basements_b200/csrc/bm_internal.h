@@ -1,4 +1,8 @@
 // bm_internal.h — shared host/device definitions of the B200 MPM library.
+//
+// Every kernel works on a table of scenes (SceneTable): the plain solver is a
+// table of one scene, the batched and served forms hold many scenes of uneven
+// particle and grid counts, stepped together by the same launches.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -10,8 +14,13 @@
 
 namespace bm {
 
-// Device-side error bits, OR-ed into the solver's status word.
+// Device-side error bits, OR-ed into a scene's status word.
 enum : uint32_t { ERR_ESCAPE = 1u, ERR_NONFINITE = 2u };
+
+// Threads per CTA of every per-particle kernel except the fused one (the
+// CTA -> scene prefix table is built for this size; the fused kernel's
+// variants use multiples of it).
+constexpr int kParticleCTA = 128;
 
 // Particle planes of the SoA store (each plane holds `cap` floats).
 enum Plane : int {
@@ -94,10 +103,39 @@ struct GridAcc {
     int32_t* count;     // number of entries in `list`
 };
 
-struct GridBuffers {
-    GridAcc acc;        // the buffer a kernel reads / updates
-    uint8_t* alloc;     // per block: ever touched (the reference's allocated blocks)
+// Device descriptor of one scene. Two particle stores (the sort permutes
+// from one into the other) and two grid accumulators (step n's grid and the
+// next step's P2G); which ones are current is a launch parameter.
+struct SceneDev {
+    ParticleSoA store[2];
+    GridDesc g;
+    GridAcc acc[2];
+    uint8_t* alloc;        // per block: ever touched (the reference's allocated blocks)
+    Material mat;
+    float dt;              // this scene's step
+    int32_t* key;          // per particle: sort key (local)
+    int32_t* rank;         // per particle: slot among equal keys
+    int64_t key_base;      // first key of this scene in the shared counting-sort arrays
+    uint32_t* status;      // error bits
+    unsigned long long* escaped;  // dropped stencil writes
 };
+
+struct SceneTable {
+    const SceneDev* scenes;     // device array, n_scenes entries
+    const int64_t* cta_prefix;  // n_scenes + 1: per-particle CTAs before each scene
+    int n_scenes;
+};
+
+// Scene of particle CTA `cta` (binary search of the prefix table).
+__device__ __forceinline__ int scene_of_cta(const SceneTable& t, int64_t cta) {
+    int lo = 0, hi = t.n_scenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t.cta_prefix[mid] <= cta) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 // Marks block b as holding data in `a` (appends it to the list once).
 __device__ __forceinline__ void touch_block(const GridAcc& a, int64_t b) {
@@ -125,62 +163,101 @@ __device__ __forceinline__ void mark_stencil_blocks(const GridDesc& g, const Gri
             }
 }
 
-// Kernel launchers (bm_step_kernels.cu): the split phases.
-void launch_p2g(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat,
-                uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st);
-// folded: cur.mv holds momentum + force * dt (the force channel only holds
-// the contributions of w*m <= 1e-6 particle-node pairs).
-void launch_grid_update(const GridDesc& g, const GridAcc& cur, const GridAcc& other, const Material& mat, float dt,
-                        bool folded, int64_t max_blocks, cudaStream_t st);
-void launch_g2p(const ParticleSoA& ps, const GridDesc& g, const GridBuffers& gb, const Material& mat, float dt,
-                uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st);
-
-// Particle ordering and fused G2P + next P2G (bm_fused.cu). Particles are
-// sorted by their stencil base node (key = flat node index of
-// floor(x/dx - 0.5); nkeys = num_nodes is the "outside the box" key).
-struct BinBuffers {
-    int32_t* key;        // per particle: key
-    int32_t* rank;       // per particle: slot among particles with the same key
-    int32_t* count;      // nkeys + 1
-    int32_t* start;      // nkeys + 2 (exclusive scan)
+// Shared arrays of the counting sort (keys of all scenes, scene by scene:
+// scene s owns keys [key_base, key_base + nodes + 1), the last one for
+// particles outside its box).
+struct SortBuffers {
+    int32_t* count;      // nkeys
+    int32_t* start;      // nkeys + 1
     int64_t* tile_sum;   // per scan tile
-    int64_t nkeys;       // real keys (= grid nodes)
-    int64_t key_cap;     // capacity of key / rank
+    int64_t nkeys;
 };
 int64_t scan_tiles(int64_t nkeys);
-void launch_bin_sort(const ParticleSoA& src, const ParticleSoA& dst, const GridDesc& g, const BinBuffers& bb,
-                     cudaStream_t st);
-void launch_g2p2g(const ParticleSoA& ps, const GridDesc& g, const GridAcc& cur, const GridAcc& next,
-                  uint8_t* alloc, const Material& mat, float dt, float dt_next, bool fast_math,
-                  uint32_t* d_status, unsigned long long* d_escaped, cudaStream_t st);
 
-// M1 PIC-rigid coupler; accumulates into d_acc (6 doubles + 1 count as double).
+// ---- launchers (bm_kernels.cu) ----------------------------------------------------
+// cur = accumulation buffer of the current step; sel = current particle store;
+// n_ctas = per-particle CTAs of the table (cta_prefix[n_scenes]).
+void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st);
+// folded: acc[cur].mv holds momentum + force * dt (the force channel only
+// holds the contributions of w*m <= 1e-6 particle-node pairs).
+void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st);
+void launch_g2p(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st);
+// Fused G2P of this step + P2G of the next (into acc[1-cur]), in one of the
+// compiled launch shapes.
+int fused_variant_count();
+const char* fused_variant_name(int v);
+// The fused kernel's view of one scene with the buffer choice (cur, sel)
+// resolved: exactly the fields it touches, no runtime-indexed arrays.
+struct FusedScene {
+    float* base;          // store[sel] planes
+    int64_t cap, n;
+    GridDesc g;
+    const float4* cur_mv;  // acc[cur].mv: this step's grid velocities
+    GridAcc next;          // acc[1-cur]: the next step's P2G
+    uint8_t* alloc;
+    float mu, lambda, neg_alpha_koh, dt;
+    uint32_t* status;
+    unsigned long long* escaped;
+    __host__ __device__ __forceinline__ float* plane(int p) const { return base + (int64_t)p * cap; }
+};
+FusedScene fused_view(const SceneDev& d, int cur, int sel);
+// Single scene, its view passed by value; many scenes, a device array of
+// views (one per scene) for this (cur, sel) and the table's CTA prefix.
+void launch_g2p2g_one(const FusedScene& scene, bool fast_math, int variant, cudaStream_t st);
+void launch_g2p2g_many(const FusedScene* d_views, const int64_t* d_prefix, int n_scenes, int64_t n_ctas,
+                       bool fast_math, int variant, cudaStream_t st);
+// Counting sort of every scene's particles by stencil base node, from
+// store[sel] into store[1-sel].
+void launch_sort(const SceneTable& t, int64_t n_ctas, int sel, const SortBuffers& sb, cudaStream_t st);
+void launch_gather_rows(const ParticleSoA& ps, int plane0, int width, float* out_add_order, cudaStream_t st);
+void launch_scatter_rows(const ParticleSoA& ps, int plane0, int width, const float* in_rows, int64_t first,
+                         int64_t n, const int32_t* inv, cudaStream_t st);
+void launch_inverse_pid(const ParticleSoA& ps, int32_t* inv, cudaStream_t st);
+
+// ---- coupler and bodies (bm_m1.cu) ------------------------------------------------
+// M1 parameters of one body for one step, computed on the host
+// (m1_prepare) or on the device from the body state (batched form).
 struct M1Params {
-    float R[9];          // body-to-world rotation, row-major (host float, no FMA)
+    float R[9];          // body-to-world rotation, row-major
     float c[3], vl[3], w[3];
     float he[3];
     float lo[3], hi[3];  // world AABB of the box formula
     float mb;            // per-node body mass
     float mb_over_dt;
     int shape;
+    int scene;           // scene whose grid the body couples to
+    int active;          // 0: dt <= 0 or AABB outside the box -> no work
     int bi0, bj0, bk0, nbi, nbj, nbk;  // candidate block range (relative to box)
 };
-bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, M1Params* out);
-void launch_m1(const GridDesc& g, const GridBuffers& gb, const M1Params& p, double* d_acc, cudaStream_t st);
+bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* out);
+// Candidate blocks the AABB of a body with these half extents can span.
+int64_t m1_max_candidates(const GridDesc& g, const float half_extents[3]);
+// One CTA of 64 threads per candidate block: grid (max_candidates, n_bodies).
+void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int64_t max_candidates, int cur,
+               double* d_acc, cudaStream_t st);
 void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st);
 
-// Dense (i,j,k) copies between the blocked device layout and host order.
-void launch_grid_to_dense(const GridDesc& g, const GridBuffers& gb, float* vel, float* force, float* mass,
-                          uint8_t* active, uint8_t* balloc, cudaStream_t st);
-void launch_dense_velocity_to_grid(const GridDesc& g, const GridBuffers& gb, const float* vel, cudaStream_t st);
-void launch_seed_grid(const GridDesc& g, const GridBuffers& gb, int64_t n, const int32_t* ijk, const float* vel,
-                      const float* mass, uint32_t* d_status, cudaStream_t st);
+// Rigid bodies stepped on the device (batched and served forms), with the
+// semi-implicit Euler update of include/basements/physics/dynamics/integrator.h:19-57.
+struct BodyDev {
+    bm_collider_t state;   // pose, velocities, extents, mass, shape
+    float inv_mass;
+    float inv_inertia[9];  // body-space inverse inertia (the reference integrator uses it as is)
+    float gravity[3];
+    float dt;
+    int32_t dynamic;       // 0: kinematic (pose advanced by the velocities only)
+    int32_t scene;
+};
+void launch_body_prepare(const SceneTable& t, const BodyDev* d_bodies, int n_bodies, M1Params* d_params,
+                         cudaStream_t st);
+void launch_body_integrate(BodyDev* d_bodies, int n_bodies, const double* d_acc, cudaStream_t st);
 
-// Particle rows in add order <-> stored order.
-void launch_gather_rows(const ParticleSoA& ps, int plane0, int width, float* out_add_order, cudaStream_t st);
-void launch_scatter_rows(const ParticleSoA& ps, int plane0, int width, const float* in_rows, int64_t first,
-                         int64_t n, const int32_t* inv, cudaStream_t st);
-void launch_inverse_pid(const ParticleSoA& ps, int32_t* inv, cudaStream_t st);
+// Dense (i,j,k) copies of one scene's grid (plain API).
+void launch_grid_to_dense(const GridDesc& g, const GridAcc& a, const uint8_t* alloc, float* vel, float* force,
+                          float* mass, uint8_t* active, uint8_t* balloc, cudaStream_t st);
+void launch_dense_velocity_to_grid(const GridDesc& g, const GridAcc& a, const float* vel, cudaStream_t st);
+void launch_seed_grid(const GridDesc& g, const GridAcc& a, uint8_t* alloc, int64_t n, const int32_t* ijk,
+                      const float* vel, const float* mass, uint32_t* d_status, cudaStream_t st);
 
 // Thread-local error text.
 void set_last_error(const std::string& s);

@@ -1,0 +1,792 @@
+// bm_kernels.cu — the MLS-MPM step kernels, over a table of scenes.
+//
+// Reference (2nugu/basements, include/basements/physics/mpm/mpm_solver.h):
+//   step :71-87   p2g_single :168-248   update_grid :250-291
+//   g2p_single :293-348   apply_plasticity :114-166
+//
+// Layout: particles are FP32 SoA planes (bm_internal.h, Plane); the grid is a
+// dense box per scene with two float4 per node: (momentum, mass) and
+// (force, 0). P2G scatters with 16-byte vector reductions into L2
+// (red.global.add.v4.f32).
+//
+// Per-particle kernels map a CTA (or a 128-thread unit of it) to its scene by
+// a binary search of the table's CTA prefix, so one launch covers scenes of
+// any particle count; the grid update takes one grid row per scene.
+//
+// Step n of MPMSolver::step runs P2G(n), update_grid(n), G2P(n). P2G(n+1)
+// only needs the particle state that G2P(n) produces, so the fused kernel
+// k_g2p2g does G2P(n) and P2G(n+1) back to back while the particle is in
+// registers: every particle is read once (x, F, m, V0) and written once
+// (x, v, C, F) per step, and the Kirchhoff stress of P2G(n+1) comes from the
+// SVD that the Drucker-Prager projection of G2P(n) already computed
+// (F_new = U S V^T with known U and S), saving the reference's second SVD.
+// Particles are kept in the order of their stencil base node
+// floor(x/dx - 0.5) (grid order, k fastest) by a counting sort
+// (warp-aggregated histogram, three-phase scan, permutation) that runs every
+// few steps, so neighbouring threads share stencil nodes: the gather hits L1
+// and a warp's reductions land on a few L2 lines. (A variant that
+// accumulated each 4^3 bin's P2G in a shared-memory tile was 3.6x slower on
+// B200: float atomics on shared memory are a compare-and-swap loop, and the
+// per-bin barriers stalled the warps.)
+#include <algorithm>
+
+#include "bm_internal.h"
+#include "bm_math.cuh"
+
+namespace bm {
+
+namespace {
+
+constexpr int kGridThreads = 256;
+constexpr int kScanThreads = 1024;
+constexpr int kScanTile = kScanThreads * 8;
+
+__device__ __forceinline__ void red_v4(float4* a, float x, float y, float z, float w) {
+    atomicAdd(a, make_float4(x, y, z, w));
+}
+
+// a[i] for a runtime i in {0,1,2} without indexing (keeps `a` in registers).
+__device__ __forceinline__ float pick3(const float a[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
+
+__device__ __forceinline__ void report(const SceneDev& S, int dropped, bool finite) {
+    if (!finite) atomicOr(S.status, ERR_NONFINITE);
+    if (dropped) {
+        atomicOr(S.status, ERR_ESCAPE);
+        atomicAdd(S.escaped, (unsigned long long)dropped);
+    }
+}
+
+// Particle handled by this thread: scene index and slot, or false.
+struct PSlot {
+    int s;
+    int64_t p;
+};
+__device__ __forceinline__ bool particle_slot(const SceneTable& t, int sel, PSlot& out) {
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t unit = gtid / kParticleCTA;
+    if (unit >= t.cta_prefix[t.n_scenes]) return false;
+    const int s = scene_of_cta(t, unit);
+    const int64_t p = (unit - t.cta_prefix[s]) * kParticleCTA + (gtid % kParticleCTA);
+    if (p >= t.scenes[s].store[sel].n) return false;
+    out.s = s;
+    out.p = p;
+    return true;
+}
+
+// ---- standalone P2G (grid.clear() + the P2G loop) --------------------------------
+
+__global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int sel) {
+    PSlot slot;
+    if (!particle_slot(t, sel, slot)) return;
+    const SceneDev& S = t.scenes[slot.s];
+    const ParticleSoA ps = S.store[sel];
+    const GridDesc g = S.g;
+    const GridAcc acc = S.acc[cur];
+    const int64_t p = slot.p;
+    const float x[3] = {ps.plane(P_X)[p], ps.plane(P_X + 1)[p], ps.plane(P_X + 2)[p]};
+    const float v[3] = {ps.plane(P_V)[p], ps.plane(P_V + 1)[p], ps.plane(P_V + 2)[p]};
+    float F[9], Cm[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        F[q] = ps.plane(P_F + q)[p];
+        Cm[q] = ps.plane(P_C + q)[p];
+    }
+    const float m = ps.plane(P_M)[p];
+    const float vol = ps.plane(P_V0)[p];
+
+    float fx[3], wgt[3][3];
+    int base[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        fx[a] = x[a] * g.inv_dx - 0.5f;
+        base[a] = (int)floorf(fx[a]);
+        bspline_weights(fx[a] - (float)base[a], wgt[a]);
+    }
+    float tau[9];
+    hencky_tau(F, S.mat.mu, S.mat.lambda, tau);
+    const float ff = -4.0f * g.inv_dx * g.inv_dx * vol;
+    float sk[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) sk[q] = tau[q] * ff;
+
+    int dropped = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float w = wgt[0][i] * wgt[1][j] * wgt[2][k];
+                if (w == 0.0f) continue;
+                const int ni = base[0] + i, nj = base[1] + j, nk = base[2] + k;
+                const float d0 = ((float)ni - fx[0] - 0.5f) * g.dx;
+                const float d1 = ((float)nj - fx[1] - 0.5f) * g.dx;
+                const float d2 = ((float)nk - fx[2] - 0.5f) * g.dx;
+                const int64_t id = g.node(ni, nj, nk);
+                if (id < 0) { ++dropped; continue; }
+                const float a0 = (Cm[0] * d0 + Cm[1] * d1) + Cm[2] * d2;
+                const float a1 = (Cm[3] * d0 + Cm[4] * d1) + Cm[5] * d2;
+                const float a2 = (Cm[6] * d0 + Cm[7] * d1) + Cm[8] * d2;
+                const float mc = w * m;
+                const float s0 = (sk[0] * d0 + sk[1] * d1) + sk[2] * d2;
+                const float s1 = (sk[3] * d0 + sk[4] * d1) + sk[5] * d2;
+                const float s2 = (sk[6] * d0 + sk[7] * d1) + sk[8] * d2;
+                red_v4(acc.mv + id, (v[0] + a0) * mc, (v[1] + a1) * mc, (v[2] + a2) * mc, mc);
+                red_v4(acc.f + id, s0 * w, s1 * w, s2 * w, 0.0f);
+            }
+    mark_stencil_blocks(g, acc, S.alloc, base, wgt[0], wgt[1], wgt[2]);
+    report(S, dropped, true);
+}
+
+// ---- grid update -------------------------------------------------------------------
+
+// update_grid over the blocks listed in acc[cur] of scene blockIdx.y (every
+// other node of the box is empty, so skipping it is exact); the same launch
+// zeroes the blocks listed in acc[1-cur] so that it can take the next P2G.
+__global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int cur, bool folded) {
+    const SceneDev& S = t.scenes[blockIdx.y];
+    const GridDesc g = S.g;
+    const GridAcc c = S.acc[cur], o = S.acc[1 - cur];
+    const Material mat = S.mat;
+    const float dt = S.dt;
+    const int n_cur = *c.count, n_other = *o.count;
+    const int64_t total = (int64_t)(n_cur + n_other) * 64;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int slot = (int)(e >> 6), tt = (int)(e & 63);
+        if (slot >= n_cur) {
+            const int64_t b = o.list[slot - n_cur];
+            const int64_t id = g.node_of_block(b, tt);
+            o.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+            o.f[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (tt == 0) o.touched[b] = 0u;
+            continue;
+        }
+        const int64_t b = c.list[slot];
+        const int64_t id = g.node_of_block(b, tt);
+        const float4 mv = c.mv[id];
+        if (!(mv.w > 1e-6f)) {
+            // inactive (mass 0) or mass <= 1e-6: the reference leaves the
+            // momentum (without force) in place (mpm_solver.h:257)
+            if (folded && (mv.w > 0.0f || mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f)) {
+                const float4 f = c.f[id];
+                c.mv[id] = make_float4(mv.x - f.x * dt, mv.y - f.y * dt, mv.z - f.z * dt, mv.w);
+            }
+            continue;
+        }
+        float v0, v1, v2;
+        if (folded) {
+            v0 = mv.x / mv.w;
+            v1 = mv.y / mv.w;
+            v2 = mv.z / mv.w;
+        } else {
+            const float4 f = c.f[id];
+            v0 = (mv.x + f.x * dt) / mv.w;
+            v1 = (mv.y + f.y * dt) / mv.w;
+            v2 = (mv.z + f.z * dt) / mv.w;
+        }
+        v0 = v0 + mat.gx * dt;
+        v1 = v1 + mat.gy * dt;
+        v2 = v2 + mat.gz * dt;
+        const int lj = (tt >> 2) & 3;
+        const int bj = (int)((b / g.nbz) % g.nby);
+        const int j = g.oy + 4 * bj + lj;
+        const float node_y = ((float)j + 0.5f) * g.dx;
+        if (node_y < g.dx && v1 < 0.0f) {
+            const float vn = -v1;
+            v1 = 0.0f;
+            const float mag = sqrtf(v0 * v0 + v2 * v2);
+            const float budget = mat.floor_friction * vn;
+            if (mag > 1e-12f) {
+                const float sc = smax(0.0f, (mag - budget) / mag);
+                v0 = v0 * sc;
+                v2 = v2 * sc;
+            }
+        }
+        c.mv[id] = make_float4(v0, v1, v2, mv.w);
+    }
+}
+
+__global__ void k_reset_counts(SceneTable t, int parity) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < t.n_scenes) *t.scenes[s].acc[parity].count = 0;
+}
+
+// ---- standalone G2P ---------------------------------------------------------------
+
+__global__ void __launch_bounds__(kParticleCTA) k_g2p(SceneTable t, int cur, int sel) {
+    PSlot slot;
+    if (!particle_slot(t, sel, slot)) return;
+    const SceneDev& S = t.scenes[slot.s];
+    const ParticleSoA ps = S.store[sel];
+    const GridDesc g = S.g;
+    const GridAcc acc = S.acc[cur];
+    const float dt = S.dt;
+    const int64_t p = slot.p;
+    float x[3] = {ps.plane(P_X)[p], ps.plane(P_X + 1)[p], ps.plane(P_X + 2)[p]};
+    float F[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) F[q] = ps.plane(P_F + q)[p];
+    float fx[3], wgt[3][3];
+    int base[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        fx[a] = x[a] * g.inv_dx - 0.5f;
+        base[a] = (int)floorf(fx[a]);
+        bspline_weights(fx[a] - (float)base[a], wgt[a]);
+    }
+    const float cs = 4.0f * g.inv_dx * g.inv_dx;
+    float v[3] = {0.0f, 0.0f, 0.0f};
+    float Cm[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Cm[q] = 0.0f;
+    int dropped = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float w = wgt[0][i] * wgt[1][j] * wgt[2][k];
+                if (w == 0.0f) continue;
+                const int ni = base[0] + i, nj = base[1] + j, nk = base[2] + k;
+                const int64_t id = g.node(ni, nj, nk);
+                if (id < 0) { ++dropped; continue; }
+                const float4 nv = acc.mv[id];
+                const float d[3] = {((float)ni - fx[0] - 0.5f) * g.dx, ((float)nj - fx[1] - 0.5f) * g.dx,
+                                    ((float)nk - fx[2] - 0.5f) * g.dx};
+                const float wv[3] = {nv.x * w, nv.y * w, nv.z * w};
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    v[a] = v[a] + wv[a];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) Cm[3 * a + c] = Cm[3 * a + c] + (wv[a] * d[c]) * cs;
+                }
+            }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) x[a] = x[a] + v[a] * dt;
+    dp_project(F, Cm, dt, S.mat.neg_alpha_koh);
+    if (x[1] < 0.0f) {
+        x[1] = 0.0f;
+        v[1] = 0.0f;
+    }
+    bool finite = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) finite = finite && isfinite(F[q]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        ps.plane(P_X + a)[p] = x[a];
+        ps.plane(P_V + a)[p] = v[a];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        ps.plane(P_F + q)[p] = F[q];
+        ps.plane(P_C + q)[p] = Cm[q];
+    }
+    report(S, dropped, finite);
+}
+
+// ---- fused G2P(n) + P2G(n+1) ------------------------------------------------------
+
+// Gather of G2P for a stencil inside the box: nodes at constant offsets from
+// the base node, loaded one k-row (3 nodes) at a time. A zero weight
+// multiplies instead of skipping, which is the same for finite grid values.
+__device__ __forceinline__ void gather_inside(const float4* __restrict__ src, int64_t EYZ, int64_t EZ,
+                                              const float wgt[3][3], const float dcs[3][3], float v[3],
+                                              float Cm[9]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float4* row = src + i * EYZ + j * EZ;
+            const float4 n[3] = {row[0], row[1], row[2]};
+            const float wij = wgt[0][i] * wgt[1][j];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float w = wij * wgt[2][k];
+                const float wv[3] = {n[k].x * w, n[k].y * w, n[k].z * w};
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    v[a] += wv[a];
+                    Cm[3 * a + 0] += wv[a] * dcs[0][i];
+                    Cm[3 * a + 1] += wv[a] * dcs[1][j];
+                    Cm[3 * a + 2] += wv[a] * dcs[2][k];
+                }
+            }
+        }
+}
+
+// One thread per particle, particles in base-node order. Reads x, F, m, V0;
+// writes x, v, C, F; scatters P2G(n+1) with one 16-byte reduction per node:
+// (momentum + force * dt, mass), the force folded in with the scene's dt. The
+// reference keeps momentum without force at nodes of mass <= 1e-6
+// (mpm_solver.h:257); every contribution to such a node has w*m <= 1e-6 on
+// its own, so exactly those contributions also add their force to the force
+// channel, and the grid update subtracts force * dt again there. A particle
+// whose 3x3x3 stencil lies inside the box (all but escaping particles)
+// addresses its nodes at constant offsets from the base node with one bounds
+// check for the whole stencil, and its affine and stress terms are summed
+// axis by axis (the three d components of a node depend on i, j and k
+// separately).
+template <bool Fast>
+__device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
+    const GridDesc& g = S.g;
+    const FusedScene& ps = S;
+    int dropped = 0;
+    float x[3] = {ps.plane(P_X)[p], ps.plane(P_X + 1)[p], ps.plane(P_X + 2)[p]};
+    float F[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) F[q] = ps.plane(P_F + q)[p];
+    const float m = ps.plane(P_M)[p];
+    const float vol = ps.plane(P_V0)[p];
+
+    // ---- G2P(n): gather velocities of the 27 stencil nodes
+    float fx[3], wgt[3][3], dd[3][3];
+    int base[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        fx[a] = x[a] * g.inv_dx - 0.5f;
+        base[a] = (int)floorf(fx[a]);
+        bspline_weights(fx[a] - (float)base[a], wgt[a]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) dd[a][i] = ((float)(base[a] + i) - fx[a] - 0.5f) * g.dx;
+    }
+    float v[3] = {0.f, 0.f, 0.f};
+    float Cm[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Cm[q] = 0.0f;
+    {
+        const float4* __restrict__ cur_mv = S.cur_mv;
+        const float cs = 4.0f * g.inv_dx * g.inv_dx;
+        const int r0 = base[0] - g.ox, r1 = base[1] - g.oy, r2 = base[2] - g.oz;
+        const bool inside = (unsigned)r0 <= (unsigned)(g.ex() - 3) && (unsigned)r1 <= (unsigned)(g.ey() - 3) &&
+                            (unsigned)r2 <= (unsigned)(g.ez() - 3);
+        if (inside) {
+            const int64_t EZ = g.ez(), EYZ = (int64_t)g.ey() * g.ez();
+            float dcs[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) dcs[a][i] = dd[a][i] * cs;
+            gather_inside(cur_mv + g.node_rel(r0, r1, r2), EYZ, EZ, wgt, dcs, v, Cm);
+        } else {
+#pragma unroll 1
+            for (int n = 0; n < 27; ++n) {
+                const int i = n / 9, j = (n / 3) % 3, k = n % 3;
+                const float w = pick3(wgt[0], i) * pick3(wgt[1], j) * pick3(wgt[2], k);
+                if (w == 0.0f) continue;
+                const int64_t id = g.node(base[0] + i, base[1] + j, base[2] + k);
+                if (id < 0) { ++dropped; continue; }
+                const float4 nv = cur_mv[id];
+                const float wv[3] = {nv.x * w, nv.y * w, nv.z * w};
+                const float d[3] = {pick3(dd[0], i), pick3(dd[1], j), pick3(dd[2], k)};
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    v[a] += wv[a];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) Cm[3 * a + c] += (wv[a] * d[c]) * cs;
+                }
+            }
+        }
+    }
+    const float dt = S.dt;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) x[a] = x[a] + v[a] * dt;
+    float U[9], lnS[3];
+    dp_project_keep<Fast>(F, Cm, dt, S.neg_alpha_koh, U, lnS);
+    if (x[1] < 0.0f) {
+        x[1] = 0.0f;
+        v[1] = 0.0f;
+    }
+    bool fin = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fin = fin && isfinite(F[q]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        ps.plane(P_X + a)[p] = x[a];
+        ps.plane(P_V + a)[p] = v[a];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        ps.plane(P_F + q)[p] = F[q];
+        ps.plane(P_C + q)[p] = Cm[q];
+    }
+
+    // ---- P2G(n+1) from the new state; tau from the projection's SVD
+    const float tr = (lnS[0] + lnS[1]) + lnS[2];
+    const float mu = S.mu, lambda = S.lambda;
+    const float td[3] = {2.0f * mu * lnS[0] + lambda * tr, 2.0f * mu * lnS[1] + lambda * tr,
+                         2.0f * mu * lnS[2] + lambda * tr};
+    float sk[9];
+    u_diag_wt(U, td, U, sk);
+    const float ff = -4.0f * g.inv_dx * g.inv_dx * vol;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) sk[q] = sk[q] * ff;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        fx[a] = x[a] * g.inv_dx - 0.5f;
+        base[a] = (int)floorf(fx[a]);
+        bspline_weights(fx[a] - (float)base[a], wgt[a]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) dd[a][i] = ((float)(base[a] + i) - fx[a] - 0.5f) * g.dx;
+    }
+    {
+        const int r0 = base[0] - g.ox, r1 = base[1] - g.oy, r2 = base[2] - g.oz;
+        const bool inside = (unsigned)r0 <= (unsigned)(g.ex() - 3) && (unsigned)r1 <= (unsigned)(g.ey() - 3) &&
+                            (unsigned)r2 <= (unsigned)(g.ez() - 3);
+        const GridAcc& next = S.next;
+        const int64_t EZ = g.ez(), EYZ = (int64_t)g.ey() * g.ez();
+        if (inside) {
+            float4* dmv = next.mv + g.node_rel(r0, r1, r2);
+            float4* df = next.f + g.node_rel(r0, r1, r2);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                // momentum direction v + C d and stress S d, summed axis by axis
+                float qi[3], si[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    qi[a] = v[a] + Cm[3 * a] * dd[0][i];
+                    si[a] = sk[3 * a] * dd[0][i];
+                }
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    float qj[3], sj[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        qj[a] = qi[a] + Cm[3 * a + 1] * dd[1][j];
+                        sj[a] = si[a] + sk[3 * a + 1] * dd[1][j];
+                    }
+                    const float wij = wgt[0][i] * wgt[1][j];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float w = wij * wgt[2][k];
+                        const float mc = w * m;
+                        const float wdt = w * dt;
+                        const int64_t off = i * EYZ + j * EZ + k;
+                        const float s0 = sj[0] + sk[2] * dd[2][k], s1 = sj[1] + sk[5] * dd[2][k],
+                                    s2 = sj[2] + sk[8] * dd[2][k];
+                        red_v4(dmv + off, (qj[0] + Cm[2] * dd[2][k]) * mc + s0 * wdt,
+                               (qj[1] + Cm[5] * dd[2][k]) * mc + s1 * wdt, (qj[2] + Cm[8] * dd[2][k]) * mc + s2 * wdt,
+                               mc);
+                        if (mc <= 1e-6f) red_v4(df + off, s0 * w, s1 * w, s2 * w, 0.0f);
+                    }
+                }
+            }
+        } else {
+#pragma unroll 1
+            for (int n = 0; n < 27; ++n) {
+                const int i = n / 9, j = (n / 3) % 3, k = n % 3;
+                const float w = pick3(wgt[0], i) * pick3(wgt[1], j) * pick3(wgt[2], k);
+                if (w == 0.0f) continue;  // mpm_solver.h:223
+                const int64_t id = g.node(base[0] + i, base[1] + j, base[2] + k);
+                if (id < 0) { ++dropped; continue; }
+                const float d0 = pick3(dd[0], i), d1 = pick3(dd[1], j), d2 = pick3(dd[2], k);
+                const float mc = w * m;
+                const float s0 = (sk[0] * d0 + sk[1] * d1) + sk[2] * d2;
+                const float s1 = (sk[3] * d0 + sk[4] * d1) + sk[5] * d2;
+                const float s2 = (sk[6] * d0 + sk[7] * d1) + sk[8] * d2;
+                const float wdt = w * dt;
+                red_v4(next.mv + id, (v[0] + ((Cm[0] * d0 + Cm[1] * d1) + Cm[2] * d2)) * mc + s0 * wdt,
+                       (v[1] + ((Cm[3] * d0 + Cm[4] * d1) + Cm[5] * d2)) * mc + s1 * wdt,
+                       (v[2] + ((Cm[6] * d0 + Cm[7] * d1) + Cm[8] * d2)) * mc + s2 * wdt, mc);
+                if (mc <= 1e-6f) red_v4(next.f + id, s0 * w, s1 * w, s2 * w, 0.0f);
+            }
+        }
+    }
+    mark_stencil_blocks(g, S.next, S.alloc, base, wgt[0], wgt[1], wgt[2]);
+    if (!fin) atomicOr(S.status, ERR_NONFINITE);
+    if (dropped) {
+        atomicOr(S.status, ERR_ESCAPE);
+        atomicAdd(S.escaped, (unsigned long long)dropped);
+    }
+}
+
+// Many scenes: the view of each 128-thread unit's scene comes from the CTA
+// prefix table.
+template <bool Fast, int Threads, int MinBlocks>
+__global__ void __launch_bounds__(Threads, MinBlocks)
+    k_g2p2g(const FusedScene* __restrict__ views, const int64_t* __restrict__ prefix, int n_scenes) {
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t unit = gtid / kParticleCTA;
+    if (unit >= prefix[n_scenes]) return;
+    int lo = 0, hi = n_scenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= unit) lo = mid;
+        else hi = mid - 1;
+    }
+    const int64_t p = (unit - prefix[lo]) * kParticleCTA + (gtid % kParticleCTA);
+    const FusedScene& S = views[lo];
+    if (p >= S.n) return;
+    g2p2g_particle<Fast>(S, p);
+}
+
+// Single scene: the view is a kernel parameter (constant bank).
+template <bool Fast, int Threads, int MinBlocks>
+__global__ void __launch_bounds__(Threads, MinBlocks) k_g2p2g_one(const __grid_constant__ FusedScene S) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.n) return;
+    g2p2g_particle<Fast>(S, p);
+}
+
+// ---- counting sort by stencil base node -------------------------------------------
+
+__device__ __forceinline__ int key_of(const GridDesc& g, const float x[3]) {
+    int r[3];
+    const int o[3] = {g.ox, g.oy, g.oz};
+    const int e[3] = {g.ex(), g.ey(), g.ez()};
+    const int outside = (int)g.num_nodes();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float f = x[a] * g.inv_dx - 0.5f;
+        if (!(f > -1e9f && f < 1e9f)) return outside;  // NaN or far outside
+        r[a] = (int)floorf(f) - o[a];
+        if ((unsigned)r[a] >= (unsigned)e[a]) return outside;
+    }
+    return (int)g.node_rel(r[0], r[1], r[2]);
+}
+
+__global__ void __launch_bounds__(kParticleCTA) k_sort_key(SceneTable t, int sel, int32_t* count) {
+    PSlot slot;
+    const bool valid = particle_slot(t, sel, slot);
+    int key = -1;
+    if (valid) {
+        const SceneDev& S = t.scenes[slot.s];
+        const ParticleSoA ps = S.store[sel];
+        const float x[3] = {ps.plane(P_X)[slot.p], ps.plane(P_X + 1)[slot.p], ps.plane(P_X + 2)[slot.p]};
+        key = (int)(S.key_base + key_of(S.g, x));
+    }
+    // warp-aggregated histogram: one atomic per distinct key in the warp
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(grp) - 1;
+    int base = 0;
+    if (valid && lane == leader) base = atomicAdd(count + key, __popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (valid) {
+        const SceneDev& S = t.scenes[slot.s];
+        S.key[slot.p] = key;
+        S.rank[slot.p] = base + __popc(grp & ((1u << lane) - 1u));
+    }
+}
+
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* s_warp, long long* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        s_warp[lane] = w;
+    }
+    __syncthreads();
+    const long long before = (warp > 0 ? s_warp[warp - 1] : 0) + x - v;
+    *total = s_warp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+// Scan phase 1: per-tile sums of count[0..n).
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int32_t* count, int64_t n, int64_t* tile_sum) {
+    const int64_t t0 = (int64_t)blockIdx.x * kScanTile;
+    long long s = 0;
+    for (int q = threadIdx.x; q < kScanTile; q += kScanThreads) {
+        const int64_t i = t0 + q;
+        if (i < n) s += count[i];
+    }
+    __shared__ long long s_warp[32];
+    long long total;
+    block_exclusive_scan(s, s_warp, &total);
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+// Scan phase 2: exclusive scan of the tile sums (one CTA).
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int64_t* tile_sum, int64_t n_tiles) {
+    __shared__ long long s_warp[32];
+    long long carry = 0;
+    for (int64_t b = 0; b < n_tiles; b += kScanThreads) {
+        const int64_t i = b + threadIdx.x;
+        const long long v = i < n_tiles ? tile_sum[i] : 0;
+        long long total;
+        const long long ex = block_exclusive_scan(v, s_warp, &total);
+        if (i < n_tiles) tile_sum[i] = carry + ex;
+        carry += total;
+    }
+}
+
+// Scan phase 3: start[i] = exclusive prefix of count; start[n] = total.
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int32_t* count, int64_t n,
+                                                             const int64_t* tile_sum, int32_t* start) {
+    const int64_t t0 = (int64_t)blockIdx.x * kScanTile;
+    constexpr int per = kScanTile / kScanThreads;
+    const int64_t i0 = t0 + (int64_t)threadIdx.x * per;
+    int32_t c[per];
+    long long s = 0;
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+        c[q] = (i0 + q < n) ? count[i0 + q] : 0;
+        s += c[q];
+    }
+    __shared__ long long s_warp[32];
+    long long total;
+    long long run = tile_sum[blockIdx.x] + block_exclusive_scan(s, s_warp, &total);
+#pragma unroll
+    for (int q = 0; q < per; ++q) {
+        if (i0 + q < n) start[i0 + q] = (int32_t)run;
+        run += c[q];
+    }
+    if (i0 + per >= n && i0 < n) start[n] = (int32_t)run;
+}
+
+// Moves each particle of store[sel] to its sorted slot of store[1-sel]
+// (slots are relative to the scene's first key).
+__global__ void __launch_bounds__(kParticleCTA) k_sort_permute(SceneTable t, int sel, const int32_t* start) {
+    PSlot slot;
+    if (!particle_slot(t, sel, slot)) return;
+    const SceneDev& S = t.scenes[slot.s];
+    const ParticleSoA src = S.store[sel], dst = S.store[1 - sel];
+    const int64_t p = slot.p;
+    const int64_t d = (int64_t)start[S.key[p]] + S.rank[p] - start[S.key_base];
+#pragma unroll
+    for (int c = 0; c < N_PLANES; ++c) dst.plane(c)[d] = src.plane(c)[p];
+    dst.pid[d] = src.pid[p];
+}
+
+// ---- particle rows in add order ------------------------------------------------
+
+__global__ void k_gather_rows(ParticleSoA ps, int plane0, int width, float* out) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ps.n) return;
+    const int64_t a = ps.pid[p];
+    for (int c = 0; c < width; ++c) out[a * width + c] = ps.plane(plane0 + c)[p];
+}
+
+__global__ void k_scatter_rows(ParticleSoA ps, int plane0, int width, const float* in, int64_t first, int64_t n,
+                               const int32_t* inv) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int64_t p = inv[first + q];
+    for (int c = 0; c < width; ++c) ps.plane(plane0 + c)[p] = in[q * width + c];
+}
+
+__global__ void k_inverse_pid(ParticleSoA ps, int32_t* inv) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ps.n) return;
+    inv[ps.pid[p]] = (int32_t)p;
+}
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Compiled launch shapes of the fused kernel: threads per CTA and the
+// minimum CTAs per SM given to the register allocator.
+struct FusedVariant {
+    const char* name;
+    int threads;
+    void (*fn[2])(const FusedScene*, const int64_t*, int);
+    void (*one[2])(const FusedScene);
+};
+
+#define BM_FUSED(T, B)                                                                               \
+    {#T "x" #B, T, {k_g2p2g<false, T, B>, k_g2p2g<true, T, B>}, {k_g2p2g_one<false, T, B>, k_g2p2g_one<true, T, B>}}
+const FusedVariant kFused[] = {
+    BM_FUSED(128, 4), BM_FUSED(128, 5), BM_FUSED(128, 6), BM_FUSED(256, 2), BM_FUSED(256, 3), BM_FUSED(64, 10),
+};
+#undef BM_FUSED
+constexpr int kNumFused = sizeof(kFused) / sizeof(kFused[0]);
+
+}  // namespace
+
+int64_t scan_tiles(int64_t nkeys) { return (nkeys + kScanTile - 1) / kScanTile; }
+
+int fused_variant_count() { return kNumFused; }
+const char* fused_variant_name(int v) { return (v >= 0 && v < kNumFused) ? kFused[v].name : "?"; }
+
+void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st) {
+    if (n_ctas <= 0) return;
+    k_p2g<<<(unsigned)n_ctas, kParticleCTA, 0, st>>>(t, cur, sel);
+}
+
+void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st) {
+    if (t.n_scenes <= 0) return;
+    const int64_t want = (2 * max_blocks * 64 + kGridThreads - 1) / kGridThreads;
+    const int64_t cap = std::max<int64_t>(4, 148 * 8 / t.n_scenes);
+    const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, cap));
+    k_grid_update<<<dim3(gx, (unsigned)t.n_scenes), kGridThreads, 0, st>>>(t, cur, folded);
+    k_reset_counts<<<nblk(t.n_scenes, 128), 128, 0, st>>>(t, 1 - cur);
+}
+
+void launch_g2p(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st) {
+    if (n_ctas <= 0) return;
+    k_g2p<<<(unsigned)n_ctas, kParticleCTA, 0, st>>>(t, cur, sel);
+}
+
+FusedScene fused_view(const SceneDev& d, int cur, int sel) {
+    FusedScene v;
+    v.base = d.store[sel].base;
+    v.cap = d.store[sel].cap;
+    v.n = d.store[sel].n;
+    v.g = d.g;
+    v.cur_mv = d.acc[cur].mv;
+    v.next = d.acc[1 - cur];
+    v.alloc = d.alloc;
+    v.mu = d.mat.mu;
+    v.lambda = d.mat.lambda;
+    v.neg_alpha_koh = d.mat.neg_alpha_koh;
+    v.dt = d.dt;
+    v.status = d.status;
+    v.escaped = d.escaped;
+    return v;
+}
+
+void launch_g2p2g_one(const FusedScene& scene, bool fast_math, int variant, cudaStream_t st) {
+    if (scene.n <= 0) return;
+    const FusedVariant& v = kFused[(variant >= 0 && variant < kNumFused) ? variant : 0];
+    v.one[fast_math ? 1 : 0]<<<nblk(scene.n, v.threads), v.threads, 0, st>>>(scene);
+}
+
+void launch_g2p2g_many(const FusedScene* d_views, const int64_t* d_prefix, int n_scenes, int64_t n_ctas,
+                       bool fast_math, int variant, cudaStream_t st) {
+    if (n_ctas <= 0 || n_scenes <= 0) return;
+    const FusedVariant& v = kFused[(variant >= 0 && variant < kNumFused) ? variant : 0];
+    v.fn[fast_math ? 1 : 0]<<<nblk(n_ctas * kParticleCTA, v.threads), v.threads, 0, st>>>(d_views, d_prefix,
+                                                                                         n_scenes);
+}
+
+void launch_sort(const SceneTable& t, int64_t n_ctas, int sel, const SortBuffers& sb, cudaStream_t st) {
+    if (n_ctas <= 0) return;
+    const int64_t n = sb.nkeys;
+    const int64_t tiles = scan_tiles(n);
+    cudaMemsetAsync(sb.count, 0, sizeof(int32_t) * n, st);
+    k_sort_key<<<(unsigned)n_ctas, kParticleCTA, 0, st>>>(t, sel, sb.count);
+    k_scan_reduce<<<(unsigned)tiles, kScanThreads, 0, st>>>(sb.count, n, sb.tile_sum);
+    k_scan_tiles<<<1, kScanThreads, 0, st>>>(sb.tile_sum, tiles);
+    k_scan_apply<<<(unsigned)tiles, kScanThreads, 0, st>>>(sb.count, n, sb.tile_sum, sb.start);
+    k_sort_permute<<<(unsigned)n_ctas, kParticleCTA, 0, st>>>(t, sel, sb.start);
+}
+
+void launch_gather_rows(const ParticleSoA& ps, int plane0, int width, float* out, cudaStream_t st) {
+    if (ps.n == 0) return;
+    k_gather_rows<<<nblk(ps.n, 256), 256, 0, st>>>(ps, plane0, width, out);
+}
+
+void launch_scatter_rows(const ParticleSoA& ps, int plane0, int width, const float* in, int64_t first, int64_t n,
+                         const int32_t* inv, cudaStream_t st) {
+    if (n == 0) return;
+    k_scatter_rows<<<nblk(n, 256), 256, 0, st>>>(ps, plane0, width, in, first, n, inv);
+}
+
+void launch_inverse_pid(const ParticleSoA& ps, int32_t* inv, cudaStream_t st) {
+    if (ps.n == 0) return;
+    k_inverse_pid<<<nblk(ps.n, 256), 256, 0, st>>>(ps, inv);
+}
+
+}  // namespace bm

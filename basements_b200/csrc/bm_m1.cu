@@ -1,18 +1,19 @@
-// bm_m1.cu — M1 PIC-rigid coupler and grid copy/seed kernels.
+// bm_m1.cu — M1 PIC-rigid coupler, device rigid-body update, grid copies.
 //
 // Reference (2nugu/basements):
 //   MPMRigidCouplerPIC::apply  include/basements/physics/coupling/mpm_rigid_coupler_pic.h:88-184
 //   shape_inside               include/basements/physics/coupling/mpm_rigid_coupler.h:90-103
 //   Matrix3::from_quaternion   include/basements/core/math/matrix3.h:432-447
+//   TimeIntegrator::integrate  include/basements/physics/dynamics/integrator.h:19-57
 //
-// One CTA of 64 threads per candidate 4^3 block of the body's AABB (one
-// thread per node). The reference visits only blocks its hash grid has
-// allocated and whose node-centre span overlaps the AABB; the same two tests
-// run here on the block-allocated flags. Node arithmetic uses explicit
-// round-to-nearest intrinsics (no FMA contraction) so that the inside test
-// and the exchanged velocities match the reference bit for bit. Force, torque
-// and the node count are reduced per CTA in double and added into a per-body
-// accumulator.
+// One CTA of 64 threads per candidate 4^3 block of a body's AABB (one thread
+// per node), one grid row per body. The reference visits only blocks its hash
+// grid has allocated and whose node-centre span overlaps the AABB; the same
+// two tests run here on the block-allocated flags. Node arithmetic is written
+// with explicit round-to-nearest operations (no FMA contraction) so that the
+// inside test and the exchanged velocities match the reference bit for bit.
+// Force, torque and the node count are reduced per CTA in double and added
+// into a per-body accumulator.
 #include <cmath>
 
 #include "bm_internal.h"
@@ -22,22 +23,110 @@ namespace bm {
 
 namespace {
 
-__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+// Round-to-nearest float arithmetic that is never contracted into FMA: the
+// intrinsics on the device, plain operators on the host (host code is built
+// with -ffp-contract=off).
+__host__ __device__ __forceinline__ float mul(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ float add(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+__host__ __device__ __forceinline__ float sub(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+__host__ __device__ __forceinline__ float dvd(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdiv_rn(a, b);
+#else
+    return a / b;
+#endif
+}
 
-__global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params P, double* acc) {
-    const int cb = blockIdx.x;
-    const int bk = P.bk0 + cb % P.nbk;
-    const int bj = P.bj0 + (cb / P.nbk) % P.nbj;
-    const int bi = P.bi0 + cb / (P.nbk * P.nbj);
-    const int64_t blin = ((int64_t)bi * g.nby + bj) * g.nbz + bk;
-    const int t = threadIdx.x;
+// mpm_rigid_coupler_pic.h:100-117 plus the candidate block range.
+__host__ __device__ bool m1_params(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* P) {
+    P->scene = scene;
+    P->active = 0;
+    P->nbi = P->nbj = P->nbk = 0;
+    P->bi0 = P->bj0 = P->bk0 = 0;
+    if (!(dt > 0.0f)) return false;
+    const float w = b.orientation[0], x = b.orientation[1], y = b.orientation[2], z = b.orientation[3];
+    const float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z), xy = mul(x, y), xz = mul(x, z), yz = mul(y, z);
+    const float wx = mul(w, x), wy = mul(w, y), wz = mul(w, z);
+    float* R = P->R;
+    R[0] = sub(1.0f, mul(2.0f, add(yy, zz))); R[1] = mul(2.0f, sub(xy, wz)); R[2] = mul(2.0f, add(xz, wy));
+    R[3] = mul(2.0f, add(xy, wz)); R[4] = sub(1.0f, mul(2.0f, add(xx, zz))); R[5] = mul(2.0f, sub(yz, wx));
+    R[6] = mul(2.0f, sub(xz, wy)); R[7] = mul(2.0f, add(yz, wx)); R[8] = sub(1.0f, mul(2.0f, add(xx, yy)));
+    const float hx = b.half_extents[0], hy = b.half_extents[1], hz = b.half_extents[2];
+    const float dx = g.dx;
+    const float vol = mul(mul(mul(8.0f, hx), hy), hz);
+    const int approx = (int)roundf(dvd(vol, mul(mul(dx, dx), dx)));
+    P->mb = dvd(b.mass, (float)(approx > 1 ? approx : 1));
+    P->mb_over_dt = dvd(P->mb, dt);
+    for (int a = 0; a < 3; ++a) {
+        const float h = add(add(mul(fabsf(R[3 * a]), hx), mul(fabsf(R[3 * a + 1]), hy)), mul(fabsf(R[3 * a + 2]), hz));
+        P->lo[a] = sub(b.center[a], h);
+        P->hi[a] = add(b.center[a], h);
+        P->c[a] = b.center[a];
+        P->vl[a] = b.linear_velocity[a];
+        P->w[a] = b.angular_velocity[a];
+        P->he[a] = b.half_extents[a];
+    }
+    P->shape = b.shape;
+    // Conservative candidate block range (the exact float test runs per block).
+    const int org[3] = {g.ox, g.oy, g.oz};
+    const int nb[3] = {g.nbx, g.nby, g.nbz};
+    int b0[3], n[3];
+    for (int a = 0; a < 3; ++a) {
+        if (!(P->lo[a] > -1e30f && P->hi[a] < 1e30f)) return false;
+        const double lo_node = floor((double)P->lo[a] / dx - 0.5) - 4;
+        const double hi_node = ceil((double)P->hi[a] / dx - 0.5) + 4;
+        double lo_b = floor((lo_node - org[a]) / 4.0);
+        double hi_b = floor((hi_node - org[a]) / 4.0);
+        lo_b = lo_b < 0.0 ? 0.0 : lo_b;
+        hi_b = hi_b > (double)(nb[a] - 1) ? (double)(nb[a] - 1) : hi_b;
+        if (hi_b < lo_b) return false;
+        b0[a] = (int)lo_b;
+        n[a] = (int)(hi_b - lo_b) + 1;
+    }
+    P->bi0 = b0[0]; P->bj0 = b0[1]; P->bk0 = b0[2];
+    P->nbi = n[0]; P->nbj = n[1]; P->nbk = n[2];
+    P->active = 1;
+    return true;
+}
+
+__global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params, int cur, double* acc_all) {
+    const M1Params& P = params[blockIdx.y];
+    if (!P.active) return;
+    const int64_t ncand = (int64_t)P.nbi * P.nbj * P.nbk;
+    const int64_t cb = blockIdx.x;
+    if (cb >= ncand) return;
+    const SceneDev& S = t.scenes[P.scene];
+    const GridDesc g = S.g;
+    const GridAcc A = S.acc[cur];
+    double* acc = acc_all + 7 * blockIdx.y;
+    const int bk = P.bk0 + (int)(cb % P.nbk);
+    const int bj = P.bj0 + (int)((cb / P.nbk) % P.nbj);
+    const int bi = P.bi0 + (int)(cb / ((int64_t)P.nbk * P.nbj));
+    const int64_t blin = g.block_of(bi, bj, bk);
+    const int tt = threadIdx.x;
 
     double f0 = 0, f1 = 0, f2 = 0, t0 = 0, t1 = 0, t2 = 0, cnt = 0;
     const int ox = g.ox + 4 * bi, oy = g.oy + 4 * bj, oz = g.oz + 4 * bk;
     const float dx = g.dx;
-    bool visit = gb.alloc[blin] != 0;
+    bool visit = S.alloc[blin] != 0;
     if (visit) {
         const float blo0 = mul((float)ox + 0.5f, dx), bhi0 = mul((float)(ox + 3) + 0.5f, dx);
         const float blo1 = mul((float)oy + 0.5f, dx), bhi1 = mul((float)(oy + 3) + 0.5f, dx);
@@ -47,8 +136,8 @@ __global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params 
         if (bhi2 < P.lo[2] || blo2 > P.hi[2]) visit = false;
     }
     if (visit) {
-        const int li = t >> 4, lj = (t >> 2) & 3, lk = t & 3;
-        const int64_t id = g.node_of_block(blin, t);
+        const int li = tt >> 4, lj = (tt >> 2) & 3, lk = tt & 3;
+        const int64_t id = g.node_of_block(blin, tt);
         const float xn[3] = {mul((float)(ox + li) + 0.5f, dx), mul((float)(oy + lj) + 0.5f, dx),
                              mul((float)(oz + lk) + 0.5f, dx)};
         const float r[3] = {sub(xn[0], P.c[0]), sub(xn[1], P.c[1]), sub(xn[2], P.c[2])};
@@ -67,7 +156,7 @@ __global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params 
             const float vb[3] = {add(P.vl[0], sub(mul(P.w[1], r[2]), mul(P.w[2], r[1]))),
                                  add(P.vl[1], sub(mul(P.w[2], r[0]), mul(P.w[0], r[2]))),
                                  add(P.vl[2], sub(mul(P.w[0], r[1]), mul(P.w[1], r[0])))};
-            float4 nv = gb.acc.mv[id];
+            float4 nv = A.mv[id];
             float va[3];
             if (!(nv.w >= 1e-9f)) {  // inactive (mass 0) or mass < 1e-9: body claims the node
                 va[0] = vb[0]; va[1] = vb[1]; va[2] = vb[2];
@@ -79,12 +168,12 @@ __global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params 
                 if (fabsf(mn) < 1e-6f) {  // Vec3 division guard of the reference
                     va[0] = va[1] = va[2] = 0.0f;
                 } else {
-                    va[0] = __fdiv_rn(pa[0], mn); va[1] = __fdiv_rn(pa[1], mn); va[2] = __fdiv_rn(pa[2], mn);
+                    va[0] = dvd(pa[0], mn); va[1] = dvd(pa[1], mn); va[2] = dvd(pa[2], mn);
                 }
                 nv = make_float4(va[0], va[1], va[2], mn);
             }
-            gb.acc.mv[id] = nv;
-            touch_block(gb.acc, blin);
+            A.mv[id] = nv;
+            touch_block(A, blin);
             const float dF[3] = {mul(sub(va[0], vb[0]), P.mb_over_dt), mul(sub(va[1], vb[1]), P.mb_over_dt),
                                  mul(sub(va[2], vb[2]), P.mb_over_dt)};
             f0 = dF[0]; f1 = dF[1]; f2 = dF[2];
@@ -101,14 +190,14 @@ __global__ void __launch_bounds__(64) k_m1(GridDesc g, GridBuffers gb, M1Params 
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
     __shared__ double part[2][7];
-    if ((t & 31) == 0) {
+    if ((tt & 31) == 0) {
 #pragma unroll
-        for (int q = 0; q < 7; ++q) part[t >> 5][q] = vals[q];
+        for (int q = 0; q < 7; ++q) part[tt >> 5][q] = vals[q];
     }
     __syncthreads();
-    if (t < 7) {
-        const double s = part[0][t] + part[1][t];
-        if (s != 0.0) atomicAdd(acc + t, s);
+    if (tt < 7) {
+        const double s = part[0][tt] + part[1][tt];
+        if (s != 0.0) atomicAdd(acc + tt, s);
     }
 }
 
@@ -125,38 +214,83 @@ __global__ void k_reaction_finalize(const double* acc, int n, bm_reaction_t* out
     out[b] = r;
 }
 
-__global__ void k_grid_to_dense(GridDesc g, GridBuffers gb, float* vel, float* force, float* mass, uint8_t* active,
-                                uint8_t* balloc) {
+__global__ void k_body_prepare(SceneTable t, const BodyDev* bodies, int n, M1Params* params) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const BodyDev& B = bodies[b];
+    m1_params(t.scenes[B.scene].g, B.state, B.dt, B.scene, params + b);
+}
+
+// integrator.h:19-57 for one body, with the body's weight applied as an
+// external force (the research harness applies m*g before the coupler,
+// bench_compare_all.cpp:97-98) and the coupler reaction added to it.
+__global__ void k_body_integrate(BodyDev* bodies, int n, const double* acc) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    BodyDev& B = bodies[b];
+    bm_collider_t& s = B.state;
+    const float dt = B.dt;
+    if (B.dynamic) {
+        const double* a = acc + 7 * b;
+        const float force[3] = {add(mul(B.gravity[0], s.mass), (float)a[0]), add(mul(B.gravity[1], s.mass), (float)a[1]),
+                                add(mul(B.gravity[2], s.mass), (float)a[2])};
+        const float torque[3] = {(float)a[3], (float)a[4], (float)a[5]};
+        for (int q = 0; q < 3; ++q)
+            s.linear_velocity[q] = add(s.linear_velocity[q], mul(mul(force[q], B.inv_mass), dt));
+        for (int q = 0; q < 3; ++q) {
+            const float it = add(add(mul(B.inv_inertia[3 * q], torque[0]), mul(B.inv_inertia[3 * q + 1], torque[1])),
+                                 mul(B.inv_inertia[3 * q + 2], torque[2]));
+            s.angular_velocity[q] = add(s.angular_velocity[q], mul(it, dt));
+        }
+    }
+    for (int q = 0; q < 3; ++q) s.center[q] = add(s.center[q], mul(s.linear_velocity[q], dt));
+    if (B.dynamic) {
+        // q += 0.5 dt (0, w) * q, then normalise (quaternion.h: Hamilton product)
+        const float qw = s.orientation[0], qx = s.orientation[1], qy = s.orientation[2], qz = s.orientation[3];
+        const float wx = s.angular_velocity[0], wy = s.angular_velocity[1], wz = s.angular_velocity[2];
+        const float dq[4] = {sub(sub(sub(mul(0.0f, qw), mul(wx, qx)), mul(wy, qy)), mul(wz, qz)),
+                             sub(add(add(mul(0.0f, qx), mul(wx, qw)), mul(wy, qz)), mul(wz, qy)),
+                             add(add(sub(mul(0.0f, qy), mul(wx, qz)), mul(wy, qw)), mul(wz, qx)),
+                             add(sub(add(mul(0.0f, qz), mul(wx, qy)), mul(wy, qx)), mul(wz, qw))};
+        const float h = mul(0.5f, dt);
+        float q[4];
+        for (int k = 0; k < 4; ++k) q[k] = add(s.orientation[k], mul(dq[k], h));
+        const float nrm = sqrtf(add(add(add(mul(q[0], q[0]), mul(q[1], q[1])), mul(q[2], q[2])), mul(q[3], q[3])));
+        if (nrm < 1e-6f) {
+            s.orientation[0] = 1.0f; s.orientation[1] = s.orientation[2] = s.orientation[3] = 0.0f;
+        } else {
+            const float inv = dvd(1.0f, nrm);
+            for (int k = 0; k < 4; ++k) s.orientation[k] = mul(q[k], inv);
+        }
+    }
+}
+
+__global__ void k_grid_to_dense(GridDesc g, GridAcc a, const uint8_t* alloc, float* vel, float* force, float* mass,
+                                uint8_t* active, uint8_t* balloc) {
     const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t ez = (int64_t)g.nbz * 4, ey = (int64_t)g.nby * 4;
-    if (q >= g.num_nodes()) return;
-    const int k = (int)(q % ez), j = (int)((q / ez) % ey), i = (int)(q / (ez * ey));
-    const int64_t id = g.node(g.ox + i, g.oy + j, g.oz + k);
-    const float4 mv = gb.acc.mv[id];
+    if (q >= g.num_nodes()) return;  // the flat layout is the dense (i,j,k) order
+    const float4 mv = a.mv[q];
     if (vel) { vel[3 * q] = mv.x; vel[3 * q + 1] = mv.y; vel[3 * q + 2] = mv.z; }
     if (force) {
-        const float4 f = gb.acc.f[id];
+        const float4 f = a.f[q];
         force[3 * q] = f.x; force[3 * q + 1] = f.y; force[3 * q + 2] = f.z;
     }
     if (mass) mass[q] = mv.w;
     if (active) active[q] = mv.w > 0.0f ? 1 : 0;
-    if (balloc) balloc[q] = gb.alloc[g.block_of_node(id)];
+    if (balloc) balloc[q] = alloc[g.block_of_node(q)];
 }
 
-__global__ void k_dense_velocity_to_grid(GridDesc g, GridBuffers gb, const float* vel) {
+__global__ void k_dense_velocity_to_grid(GridDesc g, GridAcc a, const float* vel) {
     const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t ez = (int64_t)g.nbz * 4, ey = (int64_t)g.nby * 4;
     if (q >= g.num_nodes()) return;
-    const int k = (int)(q % ez), j = (int)((q / ez) % ey), i = (int)(q / (ez * ey));
-    const int64_t id = g.node(g.ox + i, g.oy + j, g.oz + k);
-    float4 mv = gb.acc.mv[id];
+    float4 mv = a.mv[q];
     mv.x = vel[3 * q]; mv.y = vel[3 * q + 1]; mv.z = vel[3 * q + 2];
-    gb.acc.mv[id] = mv;
-    if (mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f || mv.w != 0.0f) touch_block(gb.acc, g.block_of_node(id));
+    a.mv[q] = mv;
+    if (mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f || mv.w != 0.0f) touch_block(a, g.block_of_node(q));
 }
 
-__global__ void k_seed(GridDesc g, GridBuffers gb, int64_t n, const int32_t* ijk, const float* vel, const float* mass,
-                       uint32_t* status) {
+__global__ void k_seed(GridDesc g, GridAcc a, uint8_t* alloc, int64_t n, const int32_t* ijk, const float* vel,
+                       const float* mass, uint32_t* status) {
     const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     const int64_t id = g.node(ijk[3 * q], ijk[3 * q + 1], ijk[3 * q + 2]);
@@ -164,67 +298,33 @@ __global__ void k_seed(GridDesc g, GridBuffers gb, int64_t n, const int32_t* ijk
         atomicOr(status, ERR_ESCAPE);
         return;
     }
-    gb.acc.mv[id] = make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], mass[q]);
-    gb.alloc[g.block_of_node(id)] = 1;
-    touch_block(gb.acc, g.block_of_node(id));
+    a.mv[id] = make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], mass[q]);
+    const int64_t b = g.block_of_node(id);
+    alloc[b] = 1;
+    touch_block(a, b);
 }
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
 
-// Host-side preparation in plain float (host code is compiled without FMA
-// contraction), following mpm_rigid_coupler_pic.h:100-117.
-bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, M1Params* P) {
-    if (!(dt > 0.0f)) return false;
-    const float w = b.orientation[0], x = b.orientation[1], y = b.orientation[2], z = b.orientation[3];
-    const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, xz = x * z, yz = y * z;
-    const float wx = w * x, wy = w * y, wz = w * z;
-    float* R = P->R;
-    R[0] = 1.0f - 2.0f * (yy + zz); R[1] = 2.0f * (xy - wz);        R[2] = 2.0f * (xz + wy);
-    R[3] = 2.0f * (xy + wz);        R[4] = 1.0f - 2.0f * (xx + zz); R[5] = 2.0f * (yz - wx);
-    R[6] = 2.0f * (xz - wy);        R[7] = 2.0f * (yz + wx);        R[8] = 1.0f - 2.0f * (xx + yy);
-    const float hx = b.half_extents[0], hy = b.half_extents[1], hz = b.half_extents[2];
-    const float dx = g.dx;
-    const float vol = 8.0f * hx * hy * hz;
-    const int approx = std::max(1, (int)std::round(vol / (dx * dx * dx)));
-    P->mb = b.mass / (float)approx;
-    P->mb_over_dt = P->mb / dt;
-    for (int a = 0; a < 3; ++a) {
-        const float h = std::fabs(R[3 * a]) * hx + std::fabs(R[3 * a + 1]) * hy + std::fabs(R[3 * a + 2]) * hz;
-        P->lo[a] = b.center[a] - h;
-        P->hi[a] = b.center[a] + h;
-        P->c[a] = b.center[a];
-        P->vl[a] = b.linear_velocity[a];
-        P->w[a] = b.angular_velocity[a];
-        P->he[a] = b.half_extents[a];
-    }
-    P->shape = b.shape;
-    // Conservative candidate block range (the exact float test runs per block).
-    const int org[3] = {g.ox, g.oy, g.oz};
-    const int nb[3] = {g.nbx, g.nby, g.nbz};
-    int b0[3], n[3];
-    for (int a = 0; a < 3; ++a) {
-        if (!std::isfinite(P->lo[a]) || !std::isfinite(P->hi[a])) return false;
-        const double lo_node = std::floor((double)P->lo[a] / dx - 0.5) - 4;
-        const double hi_node = std::ceil((double)P->hi[a] / dx - 0.5) + 4;
-        long lo_b = (long)std::floor((lo_node - org[a]) / 4.0);
-        long hi_b = (long)std::floor((hi_node - org[a]) / 4.0);
-        lo_b = std::max(lo_b, 0L);
-        hi_b = std::min(hi_b, (long)nb[a] - 1);
-        if (hi_b < lo_b) return false;
-        b0[a] = (int)lo_b;
-        n[a] = (int)(hi_b - lo_b + 1);
-    }
-    P->bi0 = b0[0]; P->bj0 = b0[1]; P->bk0 = b0[2];
-    P->nbi = n[0]; P->nbj = n[1]; P->nbk = n[2];
-    return true;
+bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* P) {
+    return m1_params(g, b, dt, scene, P);
 }
 
-void launch_m1(const GridDesc& g, const GridBuffers& gb, const M1Params& p, double* d_acc, cudaStream_t st) {
-    const int64_t nblocks = (int64_t)p.nbi * p.nbj * p.nbk;
-    if (nblocks <= 0) return;
-    k_m1<<<(unsigned)nblocks, 64, 0, st>>>(g, gb, p, d_acc);
+int64_t m1_max_candidates(const GridDesc& g, const float he[3]) {
+    // each AABB half side is at most hx + hy + hz (|R_ij| <= 1)
+    const double h = (double)std::fabs(he[0]) + std::fabs(he[1]) + std::fabs(he[2]);
+    const double nodes = 2.0 * h / g.dx + 12.0;
+    const int64_t per = (int64_t)std::ceil(nodes / 4.0) + 2;
+    const int64_t a = std::min<int64_t>(per, g.nbx), b = std::min<int64_t>(per, g.nby), c = std::min<int64_t>(per, g.nbz);
+    return std::max<int64_t>(1, a * b * c);
+}
+
+void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int64_t max_candidates, int cur,
+               double* d_acc, cudaStream_t st) {
+    if (n_bodies <= 0 || max_candidates <= 0) return;
+    k_m1<<<dim3((unsigned)max_candidates, (unsigned)n_bodies), 64, 0, st>>>(t, d_params, cur, d_acc);
 }
 
 void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st) {
@@ -232,19 +332,30 @@ void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* 
     k_reaction_finalize<<<nblk(n_bodies, 64), 64, 0, st>>>(d_acc, n_bodies, d_out);
 }
 
-void launch_grid_to_dense(const GridDesc& g, const GridBuffers& gb, float* vel, float* force, float* mass,
-                          uint8_t* active, uint8_t* balloc, cudaStream_t st) {
-    k_grid_to_dense<<<nblk(g.num_nodes(), 256), 256, 0, st>>>(g, gb, vel, force, mass, active, balloc);
+void launch_body_prepare(const SceneTable& t, const BodyDev* d_bodies, int n_bodies, M1Params* d_params,
+                         cudaStream_t st) {
+    if (n_bodies <= 0) return;
+    k_body_prepare<<<nblk(n_bodies, 64), 64, 0, st>>>(t, d_bodies, n_bodies, d_params);
 }
 
-void launch_dense_velocity_to_grid(const GridDesc& g, const GridBuffers& gb, const float* vel, cudaStream_t st) {
-    k_dense_velocity_to_grid<<<nblk(g.num_nodes(), 256), 256, 0, st>>>(g, gb, vel);
+void launch_body_integrate(BodyDev* d_bodies, int n_bodies, const double* d_acc, cudaStream_t st) {
+    if (n_bodies <= 0) return;
+    k_body_integrate<<<nblk(n_bodies, 64), 64, 0, st>>>(d_bodies, n_bodies, d_acc);
 }
 
-void launch_seed_grid(const GridDesc& g, const GridBuffers& gb, int64_t n, const int32_t* ijk, const float* vel,
-                      const float* mass, uint32_t* d_status, cudaStream_t st) {
+void launch_grid_to_dense(const GridDesc& g, const GridAcc& a, const uint8_t* alloc, float* vel, float* force,
+                          float* mass, uint8_t* active, uint8_t* balloc, cudaStream_t st) {
+    k_grid_to_dense<<<nblk(g.num_nodes(), 256), 256, 0, st>>>(g, a, alloc, vel, force, mass, active, balloc);
+}
+
+void launch_dense_velocity_to_grid(const GridDesc& g, const GridAcc& a, const float* vel, cudaStream_t st) {
+    k_dense_velocity_to_grid<<<nblk(g.num_nodes(), 256), 256, 0, st>>>(g, a, vel);
+}
+
+void launch_seed_grid(const GridDesc& g, const GridAcc& a, uint8_t* alloc, int64_t n, const int32_t* ijk,
+                      const float* vel, const float* mass, uint32_t* d_status, cudaStream_t st) {
     if (n <= 0) return;
-    k_seed<<<nblk(n, 256), 256, 0, st>>>(g, gb, n, ijk, vel, mass, d_status);
+    k_seed<<<nblk(n, 256), 256, 0, st>>>(g, a, alloc, n, ijk, vel, mass, d_status);
 }
 
 }  // namespace bm

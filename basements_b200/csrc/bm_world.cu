@@ -1,0 +1,393 @@
+// bm_world.cu — host core shared by the plain solver, the batch and the server.
+#include <algorithm>
+#include <cmath>
+
+#include "bm_world.h"
+
+namespace bm {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& s) { g_last_error = s; }
+const char* last_error_text() { return g_last_error.c_str(); }
+
+bm_status_t invalid_arg(const char* what) {
+    set_last_error(what);
+    return BM_ERR_INVALID_ARGUMENT;
+}
+
+bm_status_t launch_status(const char* where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_last_error(std::string(where) + ": " + cudaGetErrorString(e));
+        return BM_ERR_CUDA;
+    }
+    return BM_OK;
+}
+
+namespace {
+
+int floor_div4(int v) { return (v >= 0) ? (v / 4) : -((-v + 3) / 4); }
+
+GridDesc desc_from_domain(const bm_domain_t& d, float dx) {
+    GridDesc g{};
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = floor_div4(d.origin[a]) * 4;
+        hi[a] = (floor_div4(d.origin[a] + d.extent[a] + 3)) * 4;
+    }
+    g.ox = lo[0]; g.oy = lo[1]; g.oz = lo[2];
+    g.nbx = (hi[0] - lo[0]) / 4; g.nby = (hi[1] - lo[1]) / 4; g.nbz = (hi[2] - lo[2]) / 4;
+    g.dx = dx;
+    g.inv_dx = 1.0f / dx;
+    return g;
+}
+
+template <class T>
+bm_status_t dmalloc(T** p, size_t n, cudaStream_t st) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    BM_CHECK_CUDA(cudaMallocAsync((void**)p, sizeof(T) * n, st));
+    return BM_OK;
+}
+
+}  // namespace
+
+bm_status_t World::init() {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_last_error("no CUDA device");
+        return BM_ERR_NO_DEVICE;
+    }
+    BM_CHECK_CUDA(cudaGetDevice(&device));
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
+    BM_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    return BM_OK;
+}
+
+void World::free_scene(SceneHost& h) {
+    SceneDev& d = h.dev;
+    for (auto& s : d.store) {
+        cudaFree(s.base);
+        cudaFree(s.pid);
+        s = ParticleSoA{nullptr, nullptr, 0, 0};
+    }
+    for (auto& a : d.acc) {
+        cudaFree(a.mv);
+        cudaFree(a.f);
+        cudaFree(a.touched);
+        cudaFree(a.list);
+        cudaFree(a.count);
+        a = GridAcc{};
+    }
+    cudaFree(d.alloc);
+    cudaFree(d.key);
+    cudaFree(d.rank);
+    cudaFree(d.status);
+    cudaFree(d.escaped);
+    cudaFree(h.d_inv);
+    d.alloc = nullptr;
+    d.key = d.rank = nullptr;
+    d.status = nullptr;
+    d.escaped = nullptr;
+    h.d_inv = nullptr;
+}
+
+void World::release() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& h : scenes) free_scene(h);
+    scenes.clear();
+    cudaFree(d_scenes);
+    cudaFree(d_prefix);
+    for (auto& r : d_views)
+        for (auto& v : r) {
+            cudaFree(v);
+            v = nullptr;
+        }
+    cudaFree(sort.count);
+    cudaFree(sort.start);
+    cudaFree(sort.tile_sum);
+    d_scenes = nullptr;
+    d_prefix = nullptr;
+    sort = SortBuffers{};
+    for (auto& p : pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    pending.clear();
+    for (auto e : event_pool) cudaEventDestroy(e);
+    event_pool.clear();
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    t0 = t1 = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+}
+
+int World::add_scene() {
+    scenes.emplace_back();
+    SceneHost& h = scenes.back();
+    if (cudaMalloc((void**)&h.dev.status, sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc((void**)&h.dev.escaped, sizeof(unsigned long long)) == cudaSuccess) {
+        cudaMemsetAsync(h.dev.status, 0, sizeof(uint32_t), stream);
+        cudaMemsetAsync(h.dev.escaped, 0, sizeof(unsigned long long), stream);
+    }
+    dirty = true;
+    return (int)scenes.size() - 1;
+}
+
+Material World::material(const SceneHost& h) const {
+    Material m;
+    m.mu = h.E / (2.0f * (1.0f + h.nu));
+    m.lambda = h.E * h.nu / ((1.0f + h.nu) * (1.0f - 2.0f * h.nu));
+    const float koh = (3.0f * m.lambda + 2.0f * m.mu) / (2.0f * m.mu);
+    m.neg_alpha_koh = -h.alpha * koh;
+    m.floor_friction = h.floor_friction;
+    m.gx = h.gravity[0];
+    m.gy = h.gravity[1];
+    m.gz = h.gravity[2];
+    return m;
+}
+
+bm_status_t World::ensure_particle_capacity(SceneHost& h, int64_t need) {
+    if (need <= h.cap()) return BM_OK;
+    if (need > INT32_MAX) return invalid_arg("more than 2^31-1 particles in one scene");
+    int64_t cap = std::max<int64_t>(need, std::max<int64_t>(1024, h.cap() * 3 / 2));
+    cap = (cap + 31) / 32 * 32;
+    const int64_t n = h.n();
+    ParticleSoA fresh[2];
+    for (int s = 0; s < 2; ++s) {
+        fresh[s] = ParticleSoA{nullptr, nullptr, cap, n};
+        bm_status_t st = dmalloc(&fresh[s].base, (size_t)N_PLANES * cap, stream);
+        if (st == BM_OK) st = dmalloc(&fresh[s].pid, (size_t)cap, stream);
+        if (st != BM_OK) return st;
+    }
+    const ParticleSoA& old = h.dev.store[sel];
+    if (old.base && n > 0) {
+        for (int p = 0; p < N_PLANES; ++p)
+            BM_CHECK_CUDA(cudaMemcpyAsync(fresh[sel].plane(p), old.plane(p), sizeof(float) * n,
+                                          cudaMemcpyDeviceToDevice, stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(fresh[sel].pid, old.pid, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, stream));
+    }
+    for (auto& s : h.dev.store) {
+        if (s.base) cudaFreeAsync(s.base, stream);
+        if (s.pid) cudaFreeAsync(s.pid, stream);
+    }
+    h.dev.store[0] = fresh[0];
+    h.dev.store[1] = fresh[1];
+    for (int32_t** p : {&h.dev.key, &h.dev.rank, &h.d_inv}) {
+        if (*p) cudaFreeAsync(*p, stream);
+        bm_status_t st = dmalloc(p, (size_t)cap, stream);
+        if (st != BM_OK) return st;
+    }
+    dirty = true;
+    return BM_OK;
+}
+
+void World::update_bbox(SceneHost& h, int64_t n, const float* pos) {
+    for (int64_t p = 0; p < n; ++p)
+        for (int a = 0; a < 3; ++a) {
+            const double v = pos[3 * p + a];
+            if (!std::isfinite(v)) continue;
+            h.bbox_lo[a] = std::min(h.bbox_lo[a], v);
+            h.bbox_hi[a] = std::max(h.bbox_hi[a], v);
+        }
+}
+
+bm_status_t World::append_particles(SceneHost& h, int64_t n, const float* pos, const float* vel, const float* mass) {
+    const int64_t n0 = h.n();
+    bm_status_t st = ensure_particle_capacity(h, n0 + n);
+    if (st != BM_OK) return st;
+    std::vector<float> buf((size_t)n * N_PLANES);
+    std::vector<int32_t> pid((size_t)n);
+    auto col = [&](int p) { return buf.data() + (size_t)p * n; };
+    for (int64_t q = 0; q < n; ++q) {
+        for (int a = 0; a < 3; ++a) {
+            col(P_X + a)[q] = pos[3 * q + a];
+            col(P_V + a)[q] = vel ? vel[3 * q + a] : 0.0f;
+        }
+        for (int a = 0; a < 9; ++a) {
+            col(P_F + a)[q] = (a % 4 == 0) ? 1.0f : 0.0f;
+            col(P_C + a)[q] = 0.0f;
+        }
+        const float m = mass ? mass[q] : 1.0f;
+        col(P_M)[q] = m;
+        col(P_V0)[q] = (h.density > 1e-12f) ? (m / h.density) : 1.0f;  // mpm_solver.h:30
+        pid[q] = (int32_t)(n0 + q);
+    }
+    ParticleSoA& s = h.dev.store[sel];
+    for (int p = 0; p < N_PLANES; ++p)
+        BM_CHECK_CUDA(cudaMemcpyAsync(s.plane(p) + n0, col(p), sizeof(float) * n, cudaMemcpyHostToDevice, stream));
+    BM_CHECK_CUDA(cudaMemcpyAsync(s.pid + n0, pid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
+    BM_CHECK_CUDA(cudaStreamSynchronize(stream));
+    h.dev.store[0].n = h.dev.store[1].n = n0 + n;
+    update_bbox(h, n, pos);
+    dirty = true;
+    return BM_OK;
+}
+
+bm_status_t World::ensure_grid(SceneHost& h) {
+    if (h.grid_ready) return BM_OK;
+    if (!h.domain_set) {
+        if (h.n() == 0) return invalid_arg("grid box unknown: no particles and no domain");
+        const float dx = h.dev.g.dx;
+        bm_domain_t d;
+        for (int a = 0; a < 3; ++a) {
+            const int lo = (int)std::floor(h.bbox_lo[a] / dx - 0.5) - h.margin;
+            const int hi = (int)std::floor(h.bbox_hi[a] / dx - 0.5) + 3 + h.margin;
+            d.origin[a] = lo;
+            d.extent[a] = hi - lo;
+        }
+        h.domain = d;
+        h.domain_set = true;
+    }
+    const float dx = h.dev.g.dx;
+    GridDesc g = desc_from_domain(h.domain, dx);
+    const int64_t nn = g.num_nodes(), nb = g.num_blocks();
+    if (nn <= 0 || nn > (int64_t)INT32_MAX / 2) return invalid_arg("grid box too large or empty");
+    h.dev.g = g;
+    for (auto& a : h.dev.acc) {
+        bm_status_t st = dmalloc(&a.mv, (size_t)nn, stream);
+        if (st == BM_OK) st = dmalloc(&a.f, (size_t)nn, stream);
+        if (st == BM_OK) st = dmalloc(&a.touched, (size_t)nb, stream);
+        if (st == BM_OK) st = dmalloc(&a.list, (size_t)nb, stream);
+        if (st == BM_OK) st = dmalloc(&a.count, 1, stream);
+        if (st != BM_OK) return st;
+        BM_CHECK_CUDA(cudaMemsetAsync(a.mv, 0, sizeof(float4) * nn, stream));
+        BM_CHECK_CUDA(cudaMemsetAsync(a.f, 0, sizeof(float4) * nn, stream));
+        BM_CHECK_CUDA(cudaMemsetAsync(a.touched, 0, sizeof(uint32_t) * nb, stream));
+        BM_CHECK_CUDA(cudaMemsetAsync(a.count, 0, sizeof(int32_t), stream));
+    }
+    bm_status_t st = dmalloc(&h.dev.alloc, (size_t)nb, stream);
+    if (st != BM_OK) return st;
+    BM_CHECK_CUDA(cudaMemsetAsync(h.dev.alloc, 0, (size_t)nb, stream));
+    h.grid_ready = true;
+    dirty = true;
+    return BM_OK;
+}
+
+int64_t World::max_blocks() const {
+    int64_t m = 0;
+    for (const auto& h : scenes) m = std::max<int64_t>(m, h.dev.g.num_blocks());
+    return m;
+}
+
+bm_status_t World::sync_table() {
+    if (!dirty) return BM_OK;
+    const int ns = (int)scenes.size();
+    prefix.assign(ns + 1, 0);
+    int64_t keys = 0;
+    std::vector<SceneDev> host(ns);
+    for (int s = 0; s < ns; ++s) {
+        SceneHost& h = scenes[s];
+        h.dev.mat = material(h);
+        h.dev.key_base = keys;
+        if (h.grid_ready) keys += h.dev.g.num_nodes() + 1;
+        prefix[s + 1] = prefix[s] + (h.n() + kParticleCTA - 1) / kParticleCTA;
+        host[s] = h.dev;
+    }
+    if (keys >= (int64_t)INT32_MAX) return invalid_arg("too many grid nodes in one table");
+    if ((size_t)ns > table_cap) {
+        cudaFree(d_scenes);
+        cudaFree(d_prefix);
+        d_scenes = nullptr;
+        d_prefix = nullptr;
+        const size_t cap = std::max<size_t>(ns, table_cap * 2);
+        BM_CHECK_CUDA(cudaMalloc((void**)&d_scenes, sizeof(SceneDev) * cap));
+        BM_CHECK_CUDA(cudaMalloc((void**)&d_prefix, sizeof(int64_t) * (cap + 1)));
+        for (auto& r : d_views)
+            for (auto& v : r) {
+                cudaFree(v);
+                v = nullptr;
+                BM_CHECK_CUDA(cudaMalloc((void**)&v, sizeof(FusedScene) * cap));
+            }
+        table_cap = cap;
+    }
+    if (keys > sort_cap) {
+        cudaFree(sort.count);
+        cudaFree(sort.start);
+        cudaFree(sort.tile_sum);
+        const int64_t cap = std::max<int64_t>(keys, sort_cap * 3 / 2);
+        BM_CHECK_CUDA(cudaMalloc((void**)&sort.count, sizeof(int32_t) * cap));
+        BM_CHECK_CUDA(cudaMalloc((void**)&sort.start, sizeof(int32_t) * (cap + 1)));
+        BM_CHECK_CUDA(cudaMalloc((void**)&sort.tile_sum, sizeof(int64_t) * std::max<int64_t>(1, scan_tiles(cap))));
+        sort_cap = cap;
+    }
+    sort.nkeys = keys;
+    if (ns > 0) {
+        std::vector<FusedScene> views(ns);
+        for (int c = 0; c < 2; ++c)
+            for (int p = 0; p < 2; ++p) {
+                for (int q = 0; q < ns; ++q) views[q] = fused_view(host[q], c, p);
+                BM_CHECK_CUDA(cudaMemcpyAsync(d_views[c][p], views.data(), sizeof(FusedScene) * ns,
+                                              cudaMemcpyHostToDevice, stream));
+            }
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_scenes, host.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice, stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice,
+                                      stream));
+    }
+    dirty = false;
+    return BM_OK;
+}
+
+bm_status_t World::clear_and_p2g() {
+    timed("grid_clear", [&] {
+        for (auto& h : scenes) {
+            if (!h.grid_ready) continue;
+            const GridAcc& a = h.dev.acc[cur];
+            const int64_t nn = h.dev.g.num_nodes(), nb = h.dev.g.num_blocks();
+            cudaMemsetAsync(a.mv, 0, sizeof(float4) * nn, stream);
+            cudaMemsetAsync(a.f, 0, sizeof(float4) * nn, stream);
+            cudaMemsetAsync(a.touched, 0, sizeof(uint32_t) * nb, stream);
+            cudaMemsetAsync(a.count, 0, sizeof(int32_t), stream);
+        }
+    });
+    timed("p2g", [&] { launch_p2g(table(), n_ctas(), cur, sel, stream); });
+    return launch_status("p2g");
+}
+
+bm_status_t World::update(bool folded) {
+    timed("grid_update", [&] { launch_grid_update(table(), max_blocks(), cur, folded, stream); });
+    return launch_status("grid_update");
+}
+
+bm_status_t World::g2p() {
+    timed("g2p", [&] { launch_g2p(table(), n_ctas(), cur, sel, stream); });
+    return launch_status("g2p");
+}
+
+bm_status_t World::g2p2g(bool fast_math, int variant) {
+    timed("g2p2g", [&] {
+        if (scenes.size() == 1) {
+            SceneDev d = scenes[0].dev;
+            d.mat = material(scenes[0]);
+            launch_g2p2g_one(fused_view(d, cur, sel), fast_math, variant, stream);
+        } else {
+            launch_g2p2g_many(d_views[cur][sel], d_prefix, (int)scenes.size(), n_ctas(), fast_math, variant, stream);
+        }
+    });
+    cur = 1 - cur;
+    return launch_status("g2p2g");
+}
+
+bm_status_t World::sort_particles() {
+    timed("bin_sort", [&] { launch_sort(table(), n_ctas(), sel, sort, stream); });
+    sel = 1 - sel;
+    return launch_status("bin_sort");
+}
+
+void World::fold_pending() {
+    if (pending.empty()) return;
+    cudaEventSynchronize(pending.back().b);
+    for (auto& p : pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        slots[p.slot].total_ms += ms;
+        slots[p.slot].launches += 1;
+        event_pool.push_back(p.a);
+        event_pool.push_back(p.b);
+    }
+    pending.clear();
+}
+
+}  // namespace bm

@@ -1,0 +1,141 @@
+// bm_world.h — host core: a set of scenes on one device and one stream.
+//
+// The plain solver (bm_solver.cu) owns a World of one scene; the batched form
+// (bm_batch.cu) and the serving loop own Worlds of many scenes. A World keeps
+// each scene's device buffers, the device scene table the kernels read, and
+// the shared counting-sort arrays, and launches each phase of the step for
+// all its scenes at once.
+#pragma once
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bm_internal.h"
+
+namespace bm {
+
+#define BM_CHECK_CUDA(expr)                                                                       \
+    do {                                                                                          \
+        cudaError_t e__ = (expr);                                                                 \
+        if (e__ != cudaSuccess) {                                                                 \
+            set_last_error(std::string(#expr) + ": " + cudaGetErrorString(e__));                  \
+            return e__ == cudaErrorMemoryAllocation ? BM_ERR_OUT_OF_MEMORY : BM_ERR_CUDA;         \
+        }                                                                                         \
+    } while (0)
+
+bm_status_t invalid_arg(const char* what);
+bm_status_t launch_status(const char* where);
+
+// Host side of one scene.
+struct SceneHost {
+    SceneDev dev{};  // host copy of the device descriptor
+    // MPMSolver parameters (mpm_solver.h:100-109 defaults)
+    float E = 1.0e5f, nu = 0.3f, density = 1500.0f, alpha = 0.40f, floor_friction = 0.4f;
+    float gravity[3] = {0.0f, -9.81f, 0.0f};
+    // particle bounds seen so far (for the automatic box)
+    double bbox_lo[3] = {1e300, 1e300, 1e300}, bbox_hi[3] = {-1e300, -1e300, -1e300};
+    bool domain_set = false;
+    bm_domain_t domain{};
+    int32_t margin = 16;
+    bool grid_ready = false;
+    int32_t* d_inv = nullptr;  // add order -> stored slot (scratch of set_particles)
+    int64_t n() const { return dev.store[0].n; }
+    int64_t cap() const { return dev.store[0].cap; }
+};
+
+struct ProfileSlot {
+    const char* name;
+    double total_ms = 0;
+    int64_t launches = 0;
+};
+
+class World {
+public:
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<SceneHost> scenes;
+    int cur = 0;  // accumulation buffer of the current step
+    int sel = 0;  // current particle store
+
+    // Device table (rebuilt by sync_table when `dirty`).
+    SceneDev* d_scenes = nullptr;
+    int64_t* d_prefix = nullptr;
+    size_t table_cap = 0;
+    std::vector<int64_t> prefix;
+    bool dirty = true;
+    SortBuffers sort{};
+    int64_t sort_cap = 0;
+    FusedScene* d_views[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][sel]
+
+    // Profiling with CUDA events on the stream.
+    bool profiling = false;
+    std::vector<ProfileSlot> slots;
+    struct Pending { int slot; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+
+    bm_status_t init();
+    void release();
+
+    // Scenes.
+    int add_scene();
+    Material material(const SceneHost& h) const;
+    bm_status_t ensure_particle_capacity(SceneHost& h, int64_t need);
+    bm_status_t ensure_grid(SceneHost& h);
+    bm_status_t append_particles(SceneHost& h, int64_t n, const float* pos, const float* vel, const float* mass);
+    void update_bbox(SceneHost& h, int64_t n, const float* pos);
+    void free_scene(SceneHost& h);
+
+    // Device table.
+    bm_status_t sync_table();
+    SceneTable table() const { return SceneTable{d_scenes, d_prefix, (int)scenes.size()}; }
+    int64_t n_ctas() const { return prefix.empty() ? 0 : prefix.back(); }
+    int64_t max_blocks() const;
+
+    // Phases, for every scene of the table.
+    bm_status_t clear_and_p2g();  // grid.clear() + P2G into acc[cur]
+    bm_status_t update(bool folded);
+    bm_status_t g2p();
+    bm_status_t g2p2g(bool fast_math, int variant);  // flips cur
+    bm_status_t sort_particles();                      // flips sel
+
+    // Profiling.
+    template <class Fn>
+    void timed(const char* name, Fn&& fn);
+    void fold_pending();
+};
+
+template <class Fn>
+void World::timed(const char* name, Fn&& fn) {
+    if (!profiling) {
+        fn();
+        return;
+    }
+    int slot = -1;
+    for (size_t i = 0; i < slots.size(); ++i)
+        if (std::strcmp(slots[i].name, name) == 0) slot = (int)i;
+    if (slot < 0) {
+        slots.push_back(ProfileSlot{name});
+        slot = (int)slots.size() - 1;
+    }
+    auto get_event = [&]() {
+        cudaEvent_t e;
+        if (!event_pool.empty()) {
+            e = event_pool.back();
+            event_pool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    };
+    Pending pe{slot, get_event(), get_event()};
+    cudaEventRecord(pe.a, stream);
+    fn();
+    cudaEventRecord(pe.b, stream);
+    pending.push_back(pe);
+    if (pending.size() > 4096) fold_pending();
+}
+
+}  // namespace bm

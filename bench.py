@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--math", choices=["fast", "ieee"], default=None,
                     help="SVD arithmetic of the fused step (default: the library default)")
     ap.add_argument("--sort-interval", type=int, default=None)
+    ap.add_argument("--variant", type=int, default=None, help="launch shape of the fused kernel")
     return ap.parse_args()
 
 
@@ -170,6 +171,8 @@ def run_ours(args, ranks: Ranks):
         s.set_math_mode(args.math == "fast")
     if args.sort_interval is not None:
         s.set_sort_interval(args.sort_interval)
+    if args.variant is not None:
+        s.set_launch_variant(args.variant)
 
     def collider(step):
         return bm.make_collider(**body.at_time(step * sc.dt).as_tuple())

@@ -126,6 +126,12 @@ BM_API bm_status_t bm_solver_set_sort_interval(bm_solver_t* s, int32_t steps);
  * accuracy bars against the reference (mode 1 drifts about 2.5x further over
  * 1000 steps) and mode 1 saves under 2% of the step on B200. */
 BM_API bm_status_t bm_solver_set_math_mode(bm_solver_t* s, int32_t mode);
+/* Launch shape of the fused G2P + P2G kernel (threads per CTA x minimum
+ * CTAs per SM), one of bm_launch_variant_count(); chosen by the autotuner of
+ * the batched form or set here. */
+BM_API bm_status_t bm_solver_set_launch_variant(bm_solver_t* s, int32_t variant);
+BM_API int32_t bm_launch_variant_count(void);
+BM_API const char* bm_launch_variant_name(int32_t variant);
 /* set_material (:42-51): rescales V0 of existing particles by rho_old / rho_new. */
 BM_API bm_status_t bm_solver_set_material(bm_solver_t* s, float young_modulus, float poisson_ratio,
                                           float bulk_density);
