@@ -57,6 +57,35 @@ class ParticlesView(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_float)) for n in ("position", "velocity", "F", "C", "mass", "volume")]
 
 
+class SceneDesc(C.Structure):
+    """bm_scene_desc_t: one scene of a batch."""
+    _fields_ = [
+        ("dx", C.c_float),
+        ("has_domain", C.c_int32),
+        ("domain", Domain),
+        ("n_particles", C.c_int64),
+        ("position", C.POINTER(C.c_float)),
+        ("velocity", C.POINTER(C.c_float)),
+        ("mass", C.POINTER(C.c_float)),
+        ("young_modulus", C.c_float),
+        ("poisson_ratio", C.c_float),
+        ("bulk_density", C.c_float),
+        ("plastic_alpha", C.c_float),
+        ("floor_friction", C.c_float),
+        ("gravity", C.c_float * 3),
+        ("dt", C.c_float),
+        ("has_body", C.c_int32),
+        ("body", Collider),
+        ("body_dynamic", C.c_int32),
+        ("body_inv_inertia", C.c_float * 9),
+    ]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("sort_interval", C.c_int32), ("bin_shift", C.c_int32),
+                ("ms_per_step", C.c_float)]
+
+
 _f = C.POINTER(C.c_float)
 _i32 = C.POINTER(C.c_int32)
 _u8 = C.POINTER(C.c_uint8)
@@ -104,6 +133,21 @@ _SIGS = {
     "bm_solver_profile_read": (_st, [_h, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
                                       C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "bm_solver_profile_reset": (_st, [_h]),
+    "bm_batch_create": (_st, [C.c_int32, C.POINTER(SceneDesc), C.POINTER(_h)]),
+    "bm_batch_destroy": (_st, [_h]),
+    "bm_batch_num_scenes": (_st, [_h, C.POINTER(C.c_int32)]),
+    "bm_batch_num_particles": (_st, [_h, C.c_int32, C.POINTER(C.c_int64)]),
+    "bm_batch_step": (_st, [_h, C.c_int32]),
+    "bm_batch_steps_done": (_st, [_h, C.POINTER(C.c_int64)]),
+    "bm_batch_get_particles": (_st, [_h, C.c_int32, C.POINTER(ParticlesView)]),
+    "bm_batch_get_body": (_st, [_h, C.c_int32, C.POINTER(Collider)]),
+    "bm_batch_get_reaction": (_st, [_h, C.c_int32, C.POINTER(Reaction)]),
+    "bm_batch_sync": (_st, [_h, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "bm_batch_set_graph": (_st, [_h, C.c_int32]),
+    "bm_batch_set_launch": (_st, [_h, C.c_int32, C.c_int32, C.c_int32]),
+    "bm_batch_autotune": (_st, [_h, C.c_int32, C.POINTER(TuneResult)]),
+    "bm_batch_timer_start": (_st, [_h]),
+    "bm_batch_timer_stop": (_st, [_h, C.POINTER(C.c_double)]),
     "bm_solver_timer_start": (_st, [_h]),
     "bm_solver_timer_stop": (_st, [_h, C.POINTER(C.c_double)]),
 }
@@ -356,3 +400,113 @@ class MPMSolver:
         n = C.c_int32()
         check(lib().bm_solver_profile_read(self._h, cap, names, ms, cnt, C.byref(n)), "bm_solver_profile_read")
         return {names[i].decode(): (ms[i], cnt[i]) for i in range(n.value)}
+
+
+def scene_desc(scene, keep: list) -> SceneDesc:
+    """bm_scene_desc_t for a basements_b200.scenes.Scene; `keep` holds the
+    arrays the descriptor points to until the batch is created."""
+    d = SceneDesc()
+    d.dx = float(scene.dx)
+    if scene.domain is not None:
+        d.has_domain = 1
+        d.domain.origin[:] = [int(v) for v in scene.domain[0]]
+        d.domain.extent[:] = [int(v) for v in scene.domain[1]]
+    pos = np.ascontiguousarray(scene.position, np.float32)
+    mass = np.ascontiguousarray(scene.mass, np.float32)
+    keep += [pos, mass]
+    d.n_particles = len(pos)
+    d.position = _fp(pos)
+    d.mass = _fp(mass)
+    d.young_modulus, d.poisson_ratio, d.bulk_density = float(scene.E), float(scene.nu), float(scene.rho)
+    d.plastic_alpha, d.floor_friction = float(scene.alpha), float(scene.floor_friction)
+    d.gravity[:] = [float(v) for v in scene.gravity]
+    d.dt = float(scene.dt)
+    if scene.bodies:
+        b = scene.bodies[0]
+        d.has_body = 1
+        d.body = make_collider(**b.as_tuple())
+        d.body_dynamic = 0 if b.kinematic else 1
+    return d
+
+
+class Batch:
+    """Many scenes stepped together (bm_batch_*)."""
+
+    def __init__(self, scenes):
+        keep = []
+        descs = (SceneDesc * len(scenes))(*[scene_desc(sc, keep) for sc in scenes])
+        self._h = C.c_void_p()
+        check(lib().bm_batch_create(len(scenes), descs, C.byref(self._h)), "bm_batch_create")
+        self.n_scenes = len(scenes)
+
+    def close(self):
+        if self._h:
+            lib().bm_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n_steps=1):
+        check(lib().bm_batch_step(self._h, int(n_steps)), "bm_batch_step")
+
+    def steps_done(self):
+        n = C.c_int64()
+        check(lib().bm_batch_steps_done(self._h, C.byref(n)), "bm_batch_steps_done")
+        return n.value
+
+    def num_particles(self, scene):
+        n = C.c_int64()
+        check(lib().bm_batch_num_particles(self._h, int(scene), C.byref(n)), "bm_batch_num_particles")
+        return n.value
+
+    def get_particles(self, scene, fields=("position", "velocity", "F", "C")):
+        n = self.num_particles(scene)
+        shapes = {"position": (n, 3), "velocity": (n, 3), "F": (n, 3, 3), "C": (n, 3, 3), "mass": (n,),
+                  "volume": (n,)}
+        out = {k: np.empty(shapes[k], np.float32) for k in fields}
+        v = ParticlesView()
+        for k in out:
+            setattr(v, k, _fp(out[k]))
+        check(lib().bm_batch_get_particles(self._h, int(scene), C.byref(v)), "bm_batch_get_particles")
+        return out
+
+    def get_body(self, scene) -> Collider:
+        c = Collider()
+        check(lib().bm_batch_get_body(self._h, int(scene), C.byref(c)), "bm_batch_get_body")
+        return c
+
+    def get_reaction(self, scene):
+        r = Reaction()
+        check(lib().bm_batch_get_reaction(self._h, int(scene), C.byref(r)), "bm_batch_get_reaction")
+        return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
+
+    def sync(self):
+        bad = C.c_int32()
+        esc = C.c_int64()
+        st = lib().bm_batch_sync(self._h, C.byref(bad), C.byref(esc))
+        return st, bad.value, esc.value
+
+    def set_graph(self, on: bool):
+        check(lib().bm_batch_set_graph(self._h, 1 if on else 0), "bm_batch_set_graph")
+
+    def set_launch(self, variant, sort_interval, bin_shift=0):
+        check(lib().bm_batch_set_launch(self._h, int(variant), int(sort_interval), int(bin_shift)),
+              "bm_batch_set_launch")
+
+    def autotune(self, trial_steps=16):
+        r = TuneResult()
+        check(lib().bm_batch_autotune(self._h, int(trial_steps), C.byref(r)), "bm_batch_autotune")
+        return {"variant": r.variant, "sort_interval": r.sort_interval, "bin_shift": r.bin_shift,
+                "ms_per_step": r.ms_per_step}
+
+    def timer_start(self):
+        check(lib().bm_batch_timer_start(self._h), "bm_batch_timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        check(lib().bm_batch_timer_stop(self._h, C.byref(ms)), "bm_batch_timer_stop")
+        return ms.value

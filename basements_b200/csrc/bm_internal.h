@@ -116,6 +116,7 @@ struct SceneDev {
     int32_t* key;          // per particle: sort key (local)
     int32_t* rank;         // per particle: slot among equal keys
     int64_t key_base;      // first key of this scene in the shared counting-sort arrays
+    int32_t bin_shift;     // sort bins are 2^bin_shift nodes per axis (0: one cell)
     uint32_t* status;      // error bits
     unsigned long long* escaped;  // dropped stencil writes
 };
@@ -163,9 +164,16 @@ __device__ __forceinline__ void mark_stencil_blocks(const GridDesc& g, const Gri
             }
 }
 
+// Sort keys of one scene: bins of 2^bin_shift nodes per axis in grid order,
+// plus one key for particles outside the box.
+__host__ __device__ __forceinline__ int64_t sort_keys_of(const GridDesc& g, int bin_shift) {
+    const int m = (1 << bin_shift) - 1;
+    return (int64_t)((g.ex() + m) >> bin_shift) * ((g.ey() + m) >> bin_shift) * ((g.ez() + m) >> bin_shift) + 1;
+}
+
 // Shared arrays of the counting sort (keys of all scenes, scene by scene:
-// scene s owns keys [key_base, key_base + nodes + 1), the last one for
-// particles outside its box).
+// scene s owns keys [key_base, key_base + sort_keys_of(g, bin_shift)), the
+// last one for particles outside its box).
 struct SortBuffers {
     int32_t* count;      // nkeys
     int32_t* start;      // nkeys + 1

@@ -530,11 +530,11 @@ __global__ void __launch_bounds__(Threads, MinBlocks) k_g2p2g_one(const __grid_c
 
 // ---- counting sort by stencil base node -------------------------------------------
 
-__device__ __forceinline__ int key_of(const GridDesc& g, const float x[3]) {
+__device__ __forceinline__ int key_of(const GridDesc& g, int shift, const float x[3]) {
     int r[3];
     const int o[3] = {g.ox, g.oy, g.oz};
     const int e[3] = {g.ex(), g.ey(), g.ez()};
-    const int outside = (int)g.num_nodes();
+    const int outside = (int)sort_keys_of(g, shift) - 1;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float f = x[a] * g.inv_dx - 0.5f;
@@ -542,7 +542,9 @@ __device__ __forceinline__ int key_of(const GridDesc& g, const float x[3]) {
         r[a] = (int)floorf(f) - o[a];
         if ((unsigned)r[a] >= (unsigned)e[a]) return outside;
     }
-    return (int)g.node_rel(r[0], r[1], r[2]);
+    const int m = (1 << shift) - 1;
+    const int ey = (e[1] + m) >> shift, ez = (e[2] + m) >> shift;
+    return ((r[0] >> shift) * ey + (r[1] >> shift)) * ez + (r[2] >> shift);
 }
 
 __global__ void __launch_bounds__(kParticleCTA) k_sort_key(SceneTable t, int sel, int32_t* count) {
@@ -553,7 +555,7 @@ __global__ void __launch_bounds__(kParticleCTA) k_sort_key(SceneTable t, int sel
         const SceneDev& S = t.scenes[slot.s];
         const ParticleSoA ps = S.store[sel];
         const float x[3] = {ps.plane(P_X)[slot.p], ps.plane(P_X + 1)[slot.p], ps.plane(P_X + 2)[slot.p]};
-        key = (int)(S.key_base + key_of(S.g, x));
+        key = (int)(S.key_base + key_of(S.g, S.bin_shift, x));
     }
     // warp-aggregated histogram: one atomic per distinct key in the warp
     const unsigned grp = __match_any_sync(0xffffffffu, key);

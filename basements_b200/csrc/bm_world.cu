@@ -282,7 +282,7 @@ bm_status_t World::sync_table() {
         SceneHost& h = scenes[s];
         h.dev.mat = material(h);
         h.dev.key_base = keys;
-        if (h.grid_ready) keys += h.dev.g.num_nodes() + 1;
+        if (h.grid_ready) keys += sort_keys_of(h.dev.g, h.dev.bin_shift);
         prefix[s + 1] = prefix[s] + (h.n() + kParticleCTA - 1) / kParticleCTA;
         host[s] = h.dev;
     }

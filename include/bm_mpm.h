@@ -220,6 +220,64 @@ BM_API bm_status_t bm_solver_profile_reset(bm_solver_t* s);
 BM_API bm_status_t bm_solver_timer_start(bm_solver_t* s);
 BM_API bm_status_t bm_solver_timer_stop(bm_solver_t* s, double* ms);
 
+/* ---- batched form: many scenes per launch -------------------------------
+ * No reference counterpart (the reference steps one MPMSolver at a time,
+ * mpm_solver.h:62-87). Scenes of uneven particle and grid counts are stepped
+ * together: every phase of the step is one launch over a table of scenes,
+ * each scene with its own dx, box, material, dt and optional rigid body
+ * (coupled with M1 and integrated on the device like the reference's
+ * TimeIntegrator, integrator.h:19-57), and chunks of steps replay as one CUDA
+ * graph. */
+typedef struct bm_scene_desc {
+    float dx;
+    int32_t has_domain;          /* 0: box from the particle bounds + 16 nodes */
+    bm_domain_t domain;
+    int64_t n_particles;
+    const float* position;       /* n*3 */
+    const float* velocity;       /* n*3 or NULL */
+    const float* mass;           /* n or NULL (1.0) */
+    float young_modulus, poisson_ratio, bulk_density, plastic_alpha, floor_friction;
+    float gravity[3];
+    float dt;
+    int32_t has_body;
+    bm_collider_t body;
+    int32_t body_dynamic;        /* 0: kinematic (moved by its velocities only) */
+    float body_inv_inertia[9];   /* body-space inverse inertia; all zero = identity,
+                                    the reference scenes' value (integrator.h:33) */
+} bm_scene_desc_t;
+
+typedef struct bm_batch bm_batch_t;
+
+typedef struct bm_tune_result {
+    int32_t variant;        /* launch shape of the fused kernel */
+    int32_t sort_interval;  /* steps between regroupings */
+    int32_t bin_shift;      /* sort bins of 2^bin_shift cells per axis */
+    float ms_per_step;      /* measured with the chosen setting */
+} bm_tune_result_t;
+
+BM_API bm_status_t bm_batch_create(int32_t n_scenes, const bm_scene_desc_t* scenes, bm_batch_t** out);
+BM_API bm_status_t bm_batch_destroy(bm_batch_t* b);
+BM_API bm_status_t bm_batch_num_scenes(bm_batch_t* b, int32_t* out);
+BM_API bm_status_t bm_batch_num_particles(bm_batch_t* b, int32_t scene, int64_t* out);
+/* Every scene advances n_steps steps of its own dt. Enqueued; graph chunks
+ * replay once the launch setting is fixed. */
+BM_API bm_status_t bm_batch_step(bm_batch_t* b, int32_t n_steps);
+BM_API bm_status_t bm_batch_steps_done(bm_batch_t* b, int64_t* out);
+BM_API bm_status_t bm_batch_get_particles(bm_batch_t* b, int32_t scene, const bm_particles_view_t* view);
+BM_API bm_status_t bm_batch_get_body(bm_batch_t* b, int32_t scene, bm_collider_t* out);
+/* Reaction of the last step's coupler on the scene's body. */
+BM_API bm_status_t bm_batch_get_reaction(bm_batch_t* b, int32_t scene, bm_reaction_t* out);
+/* Waits; returns the first device-side error of any scene (and which). */
+BM_API bm_status_t bm_batch_sync(bm_batch_t* b, int32_t* bad_scene, int64_t* escaped);
+BM_API bm_status_t bm_batch_set_graph(bm_batch_t* b, int32_t on);
+BM_API bm_status_t bm_batch_set_launch(bm_batch_t* b, int32_t variant, int32_t sort_interval, int32_t bin_shift);
+/* Times each candidate launch setting for `trial_steps` steps on this batch
+ * (the state is saved before and restored after every trial, so tuning does
+ * not advance the scenes) and keeps the fastest. */
+BM_API bm_status_t bm_batch_autotune(bm_batch_t* b, int32_t trial_steps, bm_tune_result_t* out);
+BM_API bm_status_t bm_batch_timer_start(bm_batch_t* b);
+BM_API bm_status_t bm_batch_timer_stop(bm_batch_t* b, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,8 @@ def load(kind: str):
         "grid_seed": fn("grid_seed", None, C.c_void_p, C.c_int64, _i32, _f, _f),
         "box_drop_m1": fn("box_drop_m1", C.c_int, _f, C.c_int),
         "svd": fn("svd", None, C.c_int64, _f, _f, _f, _f),
+        "run_dynamic_body": fn("run_dynamic_body", None, C.c_void_p, C.POINTER(OrcCollider), C.c_float, C.c_float,
+                               C.c_float, C.c_float, C.c_int),
     }
     _loaded[kind] = api
     return api
@@ -194,6 +196,11 @@ class CpuSolver:
         r = np.zeros(6, np.float32)
         n = self.api["m1_apply"](self.h, C.byref(body), dt, _p(r))
         return r[:3].copy(), r[3:].copy(), int(n)
+
+    def run_dynamic_body(self, body: OrcCollider, gravity, dt, n_steps):
+        """n coupled steps with a dynamic body (updated in place and returned)."""
+        self.api["run_dynamic_body"](self.h, C.byref(body), *map(float, gravity), float(dt), int(n_steps))
+        return body
 
     def grid_nodes(self):
         """Every node of every allocated 4^3 block, as a dict keyed by (i,j,k)."""

@@ -62,6 +62,14 @@ ORC_EXPORT void ORC(grid_seed)(void* h, int64_t n, const int32_t* ijk, const flo
  * only: 720 steps; per step 10 floats: t, box x/y/z, box vy, p_body_y,
  * p_grid_y, p_sum_y, KE, nodes_inside. Returns the number of rows. */
 ORC_EXPORT int ORC(box_drop_m1)(float* rows, int max_rows);
+/* n coupled steps of a particle scene with one dynamic rigid body, in the
+ * order of the research harness (bench_compare_all.cpp:96-116) around the
+ * MPM phases: P2G, update_grid, weight m*g applied to the body, M1 coupler on
+ * the body's current state, reaction added, TimeIntegrator step (zero
+ * damping, identity body-space inverse inertia), G2P. body is updated in
+ * place (center, orientation, velocities). */
+ORC_EXPORT void ORC(run_dynamic_body)(void* h, orc_collider_t* body, float gx, float gy, float gz, float dt,
+                                      int n_steps);
 /* SVD of n row-major 3x3 matrices: U (n*9), sigma (n*3), V (n*9). */
 ORC_EXPORT void ORC(svd)(int64_t n, const float* F, float* U, float* S, float* V);
 

@@ -213,6 +213,45 @@ ORC_EXPORT int orc_box_drop_m1(float* rows, int max_rows) {
     return r_out;
 }
 
+ORC_EXPORT void orc_run_dynamic_body(void* h, orc_collider_t* body, float gx, float gy, float gz, float dt,
+                                     int n_steps) {
+    S* s = sv(h);
+    V3<R> pos(body->center[0], body->center[1], body->center[2]);
+    V3<R> vel(body->linear_velocity[0], body->linear_velocity[1], body->linear_velocity[2]);
+    V3<R> omg(body->angular_velocity[0], body->angular_velocity[1], body->angular_velocity[2]);
+    Q4 q{body->orientation[0], body->orientation[1], body->orientation[2], body->orientation[3]};
+    const R mass = body->mass, inv_mass = mass > R(0) ? R(1) / mass : R(0);
+    for (int i = 0; i < n_steps; ++i) {
+        s->p2g((R)dt);
+        s->update_grid((R)dt);
+        V3<R> force = V3<R>(0, 0, 0) + V3<R>((R)gx * mass, (R)gy * mass, (R)gz * mass);
+        ColliderF c = to_collider(body);
+        c.center[0] = (float)pos.x; c.center[1] = (float)pos.y; c.center[2] = (float)pos.z;
+        c.orientation[0] = (float)q.w; c.orientation[1] = (float)q.x; c.orientation[2] = (float)q.y;
+        c.orientation[3] = (float)q.z;
+        c.linear_velocity[0] = (float)vel.x; c.linear_velocity[1] = (float)vel.y; c.linear_velocity[2] = (float)vel.z;
+        c.angular_velocity[0] = (float)omg.x; c.angular_velocity[1] = (float)omg.y; c.angular_velocity[2] = (float)omg.z;
+        Reaction<R> r = m1_apply<R>(s->grid, c, (R)dt);
+        force += r.force;
+        V3<R> torque = V3<R>(0, 0, 0) + r.torque;
+        vel += force * inv_mass * (R)dt;
+        omg += (M3<R>::identity() * torque) * (R)dt;
+        pos += vel * (R)dt;
+        Q4 qv{0, omg.x, omg.y, omg.z};
+        Q4 dq = qmul(qv, q);
+        const R hh = R(0.5f) * (R)dt;
+        q = qnormalize(Q4{q.w + dq.w * hh, q.x + dq.x * hh, q.y + dq.y * hh, q.z + dq.z * hh});
+        s->g2p((R)dt);
+    }
+    body->center[0] = (float)pos.x; body->center[1] = (float)pos.y; body->center[2] = (float)pos.z;
+    body->orientation[0] = (float)q.w; body->orientation[1] = (float)q.x; body->orientation[2] = (float)q.y;
+    body->orientation[3] = (float)q.z;
+    body->linear_velocity[0] = (float)vel.x; body->linear_velocity[1] = (float)vel.y;
+    body->linear_velocity[2] = (float)vel.z;
+    body->angular_velocity[0] = (float)omg.x; body->angular_velocity[1] = (float)omg.y;
+    body->angular_velocity[2] = (float)omg.z;
+}
+
 ORC_EXPORT void orc_svd(int64_t n, const float* F, float* U, float* Sg, float* V) {
     for (int64_t q = 0; q < n; ++q) {
         M3<R> f, u, v;

@@ -196,6 +196,46 @@ ORC_EXPORT int ref_box_drop_m1(float* rows, int max_rows) {
     return r_out;
 }
 
+ORC_EXPORT void ref_run_dynamic_body(void* h, orc_collider_t* body, float gx, float gy, float gz, float dt,
+                                     int n_steps) {
+    MPMSolver* s = sv(h);
+    physics::RigidBody rb;
+    rb.make_dynamic(body->mass);
+    rb.position = Vec3(body->center[0], body->center[1], body->center[2]);
+    rb.orientation = math::Quaternion(body->orientation[0], body->orientation[1], body->orientation[2],
+                                      body->orientation[3]);
+    rb.linear_velocity = Vec3(body->linear_velocity[0], body->linear_velocity[1], body->linear_velocity[2]);
+    rb.angular_velocity = Vec3(body->angular_velocity[0], body->angular_velocity[1], body->angular_velocity[2]);
+    rb.linear_damping = 0.0f;
+    rb.angular_damping = 0.0f;
+    for (int i = 0; i < n_steps; ++i) {
+        s->grid.clear();
+        for (auto& p : s->particles) s->p2g_single(p, dt);
+        s->update_grid(dt);
+        rb.apply_force(Vec3(gx * rb.mass, gy * rb.mass, gz * rb.mass));
+        orc_collider_t c = *body;
+        c.center[0] = rb.position.x; c.center[1] = rb.position.y; c.center[2] = rb.position.z;
+        c.orientation[0] = rb.orientation.w; c.orientation[1] = rb.orientation.x;
+        c.orientation[2] = rb.orientation.y; c.orientation[3] = rb.orientation.z;
+        c.linear_velocity[0] = rb.linear_velocity.x; c.linear_velocity[1] = rb.linear_velocity.y;
+        c.linear_velocity[2] = rb.linear_velocity.z;
+        c.angular_velocity[0] = rb.angular_velocity.x; c.angular_velocity[1] = rb.angular_velocity.y;
+        c.angular_velocity[2] = rb.angular_velocity.z;
+        cp::CouplingReaction r = cp::MPMRigidCouplerPIC::apply(s->grid, to_state(&c), dt);
+        rb.force += r.force;
+        rb.torque += r.torque;
+        dynamics::TimeIntegrator::integrate(&rb, 1, dt);
+        for (auto& p : s->particles) s->g2p_single(p, dt);
+    }
+    body->center[0] = rb.position.x; body->center[1] = rb.position.y; body->center[2] = rb.position.z;
+    body->orientation[0] = rb.orientation.w; body->orientation[1] = rb.orientation.x;
+    body->orientation[2] = rb.orientation.y; body->orientation[3] = rb.orientation.z;
+    body->linear_velocity[0] = rb.linear_velocity.x; body->linear_velocity[1] = rb.linear_velocity.y;
+    body->linear_velocity[2] = rb.linear_velocity.z;
+    body->angular_velocity[0] = rb.angular_velocity.x; body->angular_velocity[1] = rb.angular_velocity.y;
+    body->angular_velocity[2] = rb.angular_velocity.z;
+}
+
 ORC_EXPORT void ref_svd(int64_t n, const float* F, float* U, float* Sg, float* V) {
     for (int64_t q = 0; q < n; ++q) {
         Matrix3 f, u, v;
