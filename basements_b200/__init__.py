@@ -86,6 +86,21 @@ class TuneResult(C.Structure):
                 ("ms_per_step", C.c_float)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_double), ("max_active", C.c_int32), ("sort_interval", C.c_int32),
+                ("variant", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("cancelled", C.c_int64), ("queued", C.c_int64), ("active", C.c_int64),
+                ("iterations", C.c_int64), ("p50_latency_ms", C.c_double), ("p99_latency_ms", C.c_double),
+                ("mean_latency_ms", C.c_double), ("particle_steps", C.c_double), ("busy_seconds", C.c_double),
+                ("peak_bytes", C.c_double)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = range(5)
+
 _f = C.POINTER(C.c_float)
 _i32 = C.POINTER(C.c_int32)
 _u8 = C.POINTER(C.c_uint8)
@@ -148,6 +163,16 @@ _SIGS = {
     "bm_batch_autotune": (_st, [_h, C.c_int32, C.POINTER(TuneResult)]),
     "bm_batch_timer_start": (_st, [_h]),
     "bm_batch_timer_stop": (_st, [_h, C.POINTER(C.c_double)]),
+    "bm_server_create": (_st, [C.POINTER(ServerConfig), C.POINTER(_h)]),
+    "bm_server_destroy": (_st, [_h]),
+    "bm_server_submit": (_st, [_h, C.POINTER(SceneDesc), C.c_int32, C.POINTER(C.c_int64)]),
+    "bm_server_poll": (_st, [_h, C.c_int64, C.POINTER(C.c_int32)]),
+    "bm_server_wait": (_st, [_h, C.c_int64, C.c_int32]),
+    "bm_server_result": (_st, [_h, C.c_int64, C.POINTER(ParticlesView), C.POINTER(Collider), C.POINTER(C.c_double)]),
+    "bm_server_release": (_st, [_h, C.c_int64]),
+    "bm_server_cancel": (_st, [_h, C.c_int64]),
+    "bm_server_stats": (_st, [_h, C.POINTER(ServerStats)]),
+    "bm_server_estimate_bytes": (_st, [C.POINTER(SceneDesc), C.POINTER(C.c_double)]),
     "bm_solver_timer_start": (_st, [_h]),
     "bm_solver_timer_stop": (_st, [_h, C.POINTER(C.c_double)]),
 }
@@ -510,3 +535,74 @@ class Batch:
         ms = C.c_double()
         check(lib().bm_batch_timer_stop(self._h, C.byref(ms)), "bm_batch_timer_stop")
         return ms.value
+
+
+class Server:
+    """Continuous-batching server (bm_server_*)."""
+
+    def __init__(self, hbm_budget_bytes=150e9, max_active=1024, sort_interval=16, variant=1):
+        cfg = ServerConfig(float(hbm_budget_bytes), int(max_active), int(sort_interval), int(variant))
+        self._h = C.c_void_p()
+        check(lib().bm_server_create(C.byref(cfg), C.byref(self._h)), "bm_server_create")
+        self._n = {}
+
+    def close(self):
+        if self._h:
+            lib().bm_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, scene, n_steps) -> int:
+        keep = []
+        d = scene_desc(scene, keep)
+        rid = C.c_int64()
+        check(lib().bm_server_submit(self._h, C.byref(d), int(n_steps), C.byref(rid)), "bm_server_submit")
+        self._n[rid.value] = scene.n
+        return rid.value
+
+    def poll(self, rid) -> int:
+        st = C.c_int32()
+        check(lib().bm_server_poll(self._h, int(rid), C.byref(st)), "bm_server_poll")
+        return st.value
+
+    def wait(self, rid, timeout_ms=60000) -> int:
+        """Returns the bm_status_t of the wait (BM_OK, BM_ERR_TIMEOUT, ...)."""
+        return lib().bm_server_wait(self._h, int(rid), int(timeout_ms))
+
+    def result(self, rid):
+        n = self._n[rid]
+        out = {"position": np.empty((n, 3), np.float32), "velocity": np.empty((n, 3), np.float32),
+               "F": np.empty((n, 3, 3), np.float32), "C": np.empty((n, 3, 3), np.float32)}
+        v = ParticlesView()
+        for k in out:
+            setattr(v, k, _fp(out[k]))
+        body = Collider()
+        lat = C.c_double()
+        check(lib().bm_server_result(self._h, int(rid), C.byref(v), C.byref(body), C.byref(lat)), "bm_server_result")
+        out["body"] = body
+        out["latency_ms"] = lat.value
+        return out
+
+    def release(self, rid):
+        check(lib().bm_server_release(self._h, int(rid)), "bm_server_release")
+
+    def cancel(self, rid):
+        check(lib().bm_server_cancel(self._h, int(rid)), "bm_server_cancel")
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().bm_server_stats(self._h, C.byref(st)), "bm_server_stats")
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+
+def estimate_bytes(scene) -> float:
+    keep = []
+    d = scene_desc(scene, keep)
+    b = C.c_double()
+    check(lib().bm_server_estimate_bytes(C.byref(d), C.byref(b)), "bm_server_estimate_bytes")
+    return b.value

@@ -117,6 +117,7 @@ struct SceneDev {
     int32_t* rank;         // per particle: slot among equal keys
     int64_t key_base;      // first key of this scene in the shared counting-sort arrays
     int32_t bin_shift;     // sort bins are 2^bin_shift nodes per axis (0: one cell)
+    int32_t fresh;         // 1: acc[cur] holds a standalone (unfolded) P2G this step
     uint32_t* status;      // error bits
     unsigned long long* escaped;  // dropped stencil writes
 };
@@ -185,9 +186,12 @@ int64_t scan_tiles(int64_t nkeys);
 // ---- launchers (bm_kernels.cu) ----------------------------------------------------
 // cur = accumulation buffer of the current step; sel = current particle store;
 // n_ctas = per-particle CTAs of the table (cta_prefix[n_scenes]).
-void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st);
+// only_fresh: skip scenes whose `fresh` flag is 0 (newly admitted scenes of
+// a running table get their first P2G while the others keep theirs).
+void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st, bool only_fresh = false);
 // folded: acc[cur].mv holds momentum + force * dt (the force channel only
-// holds the contributions of w*m <= 1e-6 particle-node pairs).
+// holds the contributions of w*m <= 1e-6 particle-node pairs); scenes whose
+// `fresh` flag is set are always treated as unfolded.
 void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st);
 void launch_g2p(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st);
 // Fused G2P of this step + P2G of the next (into acc[1-cur]), in one of the

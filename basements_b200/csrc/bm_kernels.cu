@@ -75,10 +75,11 @@ __device__ __forceinline__ bool particle_slot(const SceneTable& t, int sel, PSlo
 
 // ---- standalone P2G (grid.clear() + the P2G loop) --------------------------------
 
-__global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int sel) {
+__global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int sel, bool only_fresh) {
     PSlot slot;
     if (!particle_slot(t, sel, slot)) return;
     const SceneDev& S = t.scenes[slot.s];
+    if (only_fresh && !S.fresh) return;
     const ParticleSoA ps = S.store[sel];
     const GridDesc g = S.g;
     const GridAcc acc = S.acc[cur];
@@ -143,8 +144,9 @@ __global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int
 // update_grid over the blocks listed in acc[cur] of scene blockIdx.y (every
 // other node of the box is empty, so skipping it is exact); the same launch
 // zeroes the blocks listed in acc[1-cur] so that it can take the next P2G.
-__global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int cur, bool folded) {
+__global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int cur, bool folded_all) {
     const SceneDev& S = t.scenes[blockIdx.y];
+    const bool folded = folded_all && !S.fresh;
     const GridDesc g = S.g;
     const GridAcc c = S.acc[cur], o = S.acc[1 - cur];
     const Material mat = S.mat;
@@ -712,9 +714,9 @@ int64_t scan_tiles(int64_t nkeys) { return (nkeys + kScanTile - 1) / kScanTile; 
 int fused_variant_count() { return kNumFused; }
 const char* fused_variant_name(int v) { return (v >= 0 && v < kNumFused) ? kFused[v].name : "?"; }
 
-void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st) {
+void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st, bool only_fresh) {
     if (n_ctas <= 0) return;
-    k_p2g<<<(unsigned)n_ctas, kParticleCTA, 0, st>>>(t, cur, sel);
+    k_p2g<<<(unsigned)n_ctas, kParticleCTA, 0, st>>>(t, cur, sel, only_fresh);
 }
 
 void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st) {

@@ -1,0 +1,558 @@
+// bm_server.cu — serving loop with continuous batching.
+//
+// One worker thread owns a World (bm_world.h) of the co-resident scenes and
+// the GPU stream. Each iteration: admit queued requests in order while their
+// estimated footprint fits the HBM budget (new scenes get their first P2G
+// while the running ones keep their precomputed one), step every co-resident
+// scene together (grid update, M1 + rigid update of every body, regrouping
+// when due, fused G2P + next P2G: one launch per phase for all scenes),
+// retire the scenes that have done their steps (particles and body copied to
+// host memory) and free their device memory. Latency is measured from submit
+// to the moment the result is on the host.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "bm_world.h"
+
+using namespace bm;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct Request {
+    int64_t id = 0;
+    bm_scene_desc_t desc{};
+    std::vector<float> pos, vel, mass;
+    int32_t n_steps = 0;
+    double bytes = 0;
+    int32_t state = BM_REQ_QUEUED;
+    bm_status_t error = BM_OK;
+    bool cancel = false;
+    Clock::time_point t_submit, t_done;
+    // results
+    std::vector<float> out_pos, out_vel, out_F, out_C;
+    bm_collider_t out_body{};
+};
+
+struct Active {
+    std::shared_ptr<Request> req;
+    int32_t steps_left = 0;
+};
+
+double estimate_bytes(const bm_scene_desc_t& d) {
+    // particles: two stores of 26 floats + id, and the sort key/rank + the
+    // scratch inverse map
+    const double per_particle = 2.0 * (N_PLANES * 4 + 4) + 3 * 4;
+    double nodes = 0;
+    if (d.has_domain) {
+        nodes = 1;
+        for (int a = 0; a < 3; ++a) nodes *= (double)(d.domain.extent[a] + 8);
+    } else if (d.n_particles > 0) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int64_t p = 0; p < d.n_particles; ++p)
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = std::min(lo[a], (double)d.position[3 * p + a]);
+                hi[a] = std::max(hi[a], (double)d.position[3 * p + a]);
+            }
+        nodes = 1;
+        for (int a = 0; a < 3; ++a) nodes *= std::floor((hi[a] - lo[a]) / d.dx) + 3 + 2 * 16 + 8;
+    }
+    // two accumulators (2 float4 each), per-block flags and lists, sort keys
+    const double per_node = 2 * 32 + 8 + 17.0 / 64;
+    return per_particle * (double)d.n_particles + per_node * nodes + (1 << 16);
+}
+
+double percentile(std::vector<double> v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const double pos = q * (double)(v.size() - 1);
+    const size_t i = (size_t)std::floor(pos);
+    const double f = pos - (double)i;
+    return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+}
+
+}  // namespace
+
+struct bm_server {
+    bm_server_config_t cfg{};
+    int device = 0;
+    World w;
+    std::vector<Active> active;  // same order as w.scenes
+    // bodies of the active scenes (rebuilt when the set changes)
+    std::vector<BodyDev> h_bodies;
+    BodyDev* d_bodies = nullptr;
+    M1Params* d_params = nullptr;
+    double* d_acc = nullptr;
+    bm_reaction_t* d_react = nullptr;
+    int body_cap = 0;
+    int64_t max_cand = 0;
+    double used_bytes = 0;
+    // shared state
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::unordered_map<int64_t, std::shared_ptr<Request>> all;
+    int64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+    // stats (under mu)
+    int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, iterations = 0, n_active = 0;
+    std::vector<double> latencies;
+    double particle_steps = 0, busy = 0, peak_bytes = 0;
+};
+
+namespace {
+
+// Rebuilds the device body array from the active scenes, in scene order.
+// The current pose and velocities of each body are kept in its request
+// (save_bodies copies them back before the scene set changes).
+bm_status_t rebuild_bodies(bm_server* s) {
+    World& w = s->w;
+    std::vector<BodyDev> next;
+    s->max_cand = 0;
+    for (size_t i = 0; i < s->active.size(); ++i) {
+        const Request& r = *s->active[i].req;
+        if (!r.desc.has_body) continue;
+        BodyDev B{};
+        B.state = r.out_body;
+        B.inv_mass = r.desc.body.mass > 0.0f ? 1.0f / r.desc.body.mass : 0.0f;
+        bool zero = true;
+        for (int q = 0; q < 9; ++q) zero = zero && r.desc.body_inv_inertia[q] == 0.0f;
+        for (int q = 0; q < 9; ++q)
+            B.inv_inertia[q] = zero ? ((q % 4 == 0) ? 1.0f : 0.0f) : r.desc.body_inv_inertia[q];
+        for (int a = 0; a < 3; ++a) B.gravity[a] = r.desc.gravity[a];
+        B.dt = r.desc.dt;
+        B.dynamic = r.desc.body_dynamic;
+        B.scene = (int32_t)i;
+        next.push_back(B);
+        s->max_cand = std::max(s->max_cand, m1_max_candidates(w.scenes[i].dev.g, r.desc.body.half_extents));
+    }
+    s->h_bodies = next;
+    if ((int)next.size() > s->body_cap) {
+        cudaFree(s->d_bodies);
+        cudaFree(s->d_params);
+        cudaFree(s->d_acc);
+        cudaFree(s->d_react);
+        const int cap = std::max<int>((int)next.size(), s->body_cap * 2);
+        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_bodies, sizeof(BodyDev) * cap));
+        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_params, sizeof(M1Params) * cap));
+        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_acc, sizeof(double) * 7 * cap));
+        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_react, sizeof(bm_reaction_t) * cap));
+        s->body_cap = cap;
+    }
+    if (!next.empty())
+        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_bodies, next.data(), sizeof(BodyDev) * next.size(), cudaMemcpyHostToDevice,
+                                      w.stream));
+    BM_CHECK_CUDA(cudaStreamSynchronize(w.stream));
+    return BM_OK;
+}
+
+// Copies the device body states back into their requests (before the scene
+// set changes, so that rebuild_bodies starts from the current states).
+bm_status_t save_bodies(bm_server* s) {
+    if (s->h_bodies.empty()) return BM_OK;
+    std::vector<BodyDev> cur(s->h_bodies.size());
+    BM_CHECK_CUDA(cudaStreamSynchronize(s->w.stream));
+    BM_CHECK_CUDA(cudaMemcpy(cur.data(), s->d_bodies, sizeof(BodyDev) * cur.size(), cudaMemcpyDeviceToHost));
+    for (const BodyDev& b : cur)
+        if (b.scene >= 0 && b.scene < (int)s->active.size()) s->active[b.scene].req->out_body = b.state;
+    return BM_OK;
+}
+
+bm_status_t admit(bm_server* s, std::shared_ptr<Request> r) {
+    World& w = s->w;
+    const bm_scene_desc_t& d = r->desc;
+    w.add_scene();
+    SceneHost& h = w.scenes.back();
+    h.dev.g.dx = d.dx;
+    h.dev.g.inv_dx = 1.0f / d.dx;
+    h.dev.dt = d.dt;
+    h.dev.fresh = 1;
+    h.E = d.young_modulus;
+    h.nu = d.poisson_ratio;
+    h.density = d.bulk_density;
+    h.alpha = d.plastic_alpha;
+    h.floor_friction = d.floor_friction;
+    for (int a = 0; a < 3; ++a) h.gravity[a] = d.gravity[a];
+    if (d.has_domain) {
+        h.domain = d.domain;
+        h.domain_set = true;
+    }
+    bm_status_t st = BM_OK;
+    if (!r->pos.empty())
+        st = w.append_particles(h, (int64_t)r->mass.size(), r->pos.data(), r->vel.empty() ? nullptr : r->vel.data(),
+                                r->mass.data());
+    if (st == BM_OK) st = w.ensure_grid(h);
+    if (st != BM_OK) {
+        w.remove_scene((int)w.scenes.size() - 1);
+        return st;
+    }
+    r->out_body = d.body;
+    Active a;
+    a.req = r;
+    a.steps_left = r->n_steps;
+    s->active.push_back(a);
+    s->used_bytes += r->bytes;
+    return BM_OK;
+}
+
+// Copies a finished scene's particles (add order) and body to its request.
+bm_status_t collect(bm_server* s, int i) {
+    World& w = s->w;
+    SceneHost& h = w.scenes[i];
+    Request& r = *s->active[i].req;
+    const int64_t n = h.n();
+    r.out_pos.resize(3 * n);
+    r.out_vel.resize(3 * n);
+    r.out_F.resize(9 * n);
+    r.out_C.resize(9 * n);
+    if (n > 0) {
+        float* tmp = nullptr;
+        BM_CHECK_CUDA(cudaMallocAsync((void**)&tmp, sizeof(float) * 9 * n, w.stream));
+        const ParticleSoA& ps = h.dev.store[w.sel];
+        struct F { float* dst; int plane; int width; };
+        const F fs[] = {{r.out_pos.data(), P_X, 3}, {r.out_vel.data(), P_V, 3}, {r.out_F.data(), P_F, 9},
+                        {r.out_C.data(), P_C, 9}};
+        for (const F& f : fs) {
+            launch_gather_rows(ps, f.plane, f.width, tmp, w.stream);
+            BM_CHECK_CUDA(cudaMemcpyAsync(f.dst, tmp, sizeof(float) * f.width * n, cudaMemcpyDeviceToHost, w.stream));
+        }
+        cudaFreeAsync(tmp, w.stream);
+    }
+    uint32_t status = 0;
+    BM_CHECK_CUDA(cudaMemcpyAsync(&status, h.dev.status, sizeof(status), cudaMemcpyDeviceToHost, w.stream));
+    BM_CHECK_CUDA(cudaStreamSynchronize(w.stream));
+    r.error = (status & ERR_NONFINITE) ? BM_ERR_NON_FINITE : (status & ERR_ESCAPE) ? BM_ERR_DOMAIN_ESCAPE : BM_OK;
+    return BM_OK;
+}
+
+bm_status_t step_all(bm_server* s, bool admitted) {
+    World& w = s->w;
+    bm_status_t st = w.sync_table();
+    if (st != BM_OK) return st;
+    bool any_fresh = false;
+    for (auto& h : w.scenes) any_fresh = any_fresh || h.dev.fresh;
+    if (any_fresh) st = w.p2g_fresh();
+    if (st == BM_OK) st = w.update(true);
+    if (st == BM_OK && !s->h_bodies.empty()) {
+        const int nb = (int)s->h_bodies.size();
+        BM_CHECK_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(double) * 7 * nb, w.stream));
+        launch_body_prepare(w.table(), s->d_bodies, nb, s->d_params, w.stream);
+        launch_m1(w.table(), s->d_params, nb, s->max_cand, w.cur, s->d_acc, w.stream);
+        launch_body_integrate(s->d_bodies, nb, s->d_acc, w.stream);
+        st = launch_status("server coupler");
+    }
+    const int K = std::max(1, s->cfg.sort_interval);
+    if (st == BM_OK && (admitted || s->iterations % K == 0)) st = w.sort_particles();
+    if (st == BM_OK) st = w.g2p2g(false, s->cfg.variant);
+    for (auto& h : w.scenes)
+        if (h.dev.fresh) {
+            h.dev.fresh = 0;
+            w.dirty = true;
+        }
+    return st;
+}
+
+void worker_main(bm_server* s) {
+    cudaSetDevice(s->device);
+    World& w = s->w;
+    for (;;) {
+        std::vector<std::shared_ptr<Request>> to_admit;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            while (!s->stop && s->queue.empty() && s->active.empty())
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(100));
+            if (s->stop) break;
+            // admit in arrival order while the footprint fits
+            double used = s->used_bytes;
+            int n_active = (int)s->active.size();
+            while (!s->queue.empty()) {
+                auto r = s->queue.front();
+                if (r->cancel) {
+                    s->queue.pop_front();
+                    r->state = BM_REQ_CANCELLED;
+                    ++s->cancelled;
+                    s->cv_done.notify_all();
+                    continue;
+                }
+                if (n_active >= s->cfg.max_active) break;
+                if (used + r->bytes > s->cfg.hbm_budget_bytes && n_active > 0) break;
+                s->queue.pop_front();
+                r->state = BM_REQ_RUNNING;
+                used += r->bytes;
+                ++n_active;
+                to_admit.push_back(r);
+            }
+        }
+        const auto t0 = Clock::now();
+        bool changed = false;
+        if (!to_admit.empty()) {
+            save_bodies(s);
+            for (auto& r : to_admit) {
+                const bm_status_t st = admit(s, r);
+                if (st != BM_OK) {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    r->state = BM_REQ_FAILED;
+                    r->error = st;
+                    r->t_done = Clock::now();
+                    ++s->failed;
+                    s->cv_done.notify_all();
+                }
+            }
+            changed = true;
+            s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
+            rebuild_bodies(s);
+        }
+        if (s->active.empty()) continue;
+        bm_status_t st = step_all(s, changed);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            ++s->iterations;
+        }
+        // retire finished, cancelled or failed scenes
+        std::vector<int> done;
+        for (int i = 0; i < (int)s->active.size(); ++i) {
+            Active& a = s->active[i];
+            a.steps_left -= 1;
+            if (st != BM_OK || a.steps_left <= 0 || a.req->cancel) done.push_back(i);
+        }
+        if (!done.empty()) {
+            save_bodies(s);
+            for (int k = (int)done.size() - 1; k >= 0; --k) {
+                const int i = done[k];
+                auto r = s->active[i].req;
+                if (st == BM_OK && !r->cancel) collect(s, i);
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    r->t_done = Clock::now();
+                    if (st != BM_OK) {
+                        r->state = BM_REQ_FAILED;
+                        r->error = st;
+                        ++s->failed;
+                    } else if (r->cancel) {
+                        r->state = BM_REQ_CANCELLED;
+                        ++s->cancelled;
+                    } else {
+                        r->state = BM_REQ_DONE;
+                        ++s->completed;
+                        s->particle_steps += (double)r->mass.size() * r->n_steps;
+                        s->latencies.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+                    }
+                    r->pos.clear();
+                    r->vel.clear();
+                }
+                s->used_bytes -= r->bytes;
+                w.remove_scene(i);
+                s->active.erase(s->active.begin() + i);
+            }
+            rebuild_bodies(s);
+            s->cv_done.notify_all();
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->busy += std::chrono::duration<double>(Clock::now() - t0).count();
+            s->n_active = (int64_t)s->active.size();
+        }
+    }
+    // shutdown: cancel what is left
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (auto& r : s->queue) r->state = BM_REQ_CANCELLED;
+    for (auto& a : s->active) a.req->state = BM_REQ_CANCELLED;
+    s->queue.clear();
+    s->cv_done.notify_all();
+}
+
+}  // namespace
+
+extern "C" {
+
+BM_API bm_status_t bm_server_estimate_bytes(const bm_scene_desc_t* scene, double* bytes) {
+    if (!scene || !bytes) return invalid_arg("NULL argument");
+    *bytes = estimate_bytes(*scene);
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_create(const bm_server_config_t* config, bm_server_t** out) {
+    if (!out) return invalid_arg("out is NULL");
+    *out = nullptr;
+    bm_server* s = new bm_server();
+    s->cfg.hbm_budget_bytes = 150e9;
+    s->cfg.max_active = 1024;
+    s->cfg.sort_interval = 16;
+    s->cfg.variant = 1;
+    if (config) {
+        if (config->hbm_budget_bytes > 0) s->cfg.hbm_budget_bytes = config->hbm_budget_bytes;
+        if (config->max_active > 0) s->cfg.max_active = config->max_active;
+        if (config->sort_interval > 0) s->cfg.sort_interval = config->sort_interval;
+        if (config->variant >= 0 && config->variant < fused_variant_count()) s->cfg.variant = config->variant;
+    }
+    bm_status_t st = s->w.init();
+    if (st != BM_OK) {
+        delete s;
+        return st;
+    }
+    s->device = s->w.device;
+    s->worker = std::thread(worker_main, s);
+    *out = s;
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_destroy(bm_server_t* s) {
+    if (!s) return invalid_arg("NULL handle");
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->device);
+    s->w.release();
+    cudaFree(s->d_bodies);
+    cudaFree(s->d_params);
+    cudaFree(s->d_acc);
+    cudaFree(s->d_react);
+    delete s;
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_submit(bm_server_t* s, const bm_scene_desc_t* scene, int32_t n_steps,
+                                    int64_t* request_id) {
+    if (!s || !scene || !request_id) return invalid_arg("NULL argument");
+    if (n_steps <= 0) return invalid_arg("n_steps must be positive");
+    const bm_scene_desc_t& d = *scene;
+    if (!(d.dx > 0.0f) || !(d.dt > 0.0f)) return invalid_arg("scene dx and dt must be positive");
+    if (d.n_particles < 0 || (d.n_particles > 0 && !d.position)) return invalid_arg("bad particle arrays");
+    if (!d.has_domain && d.n_particles == 0) return invalid_arg("a scene without particles needs a domain");
+    auto r = std::make_shared<Request>();
+    r->desc = d;
+    r->n_steps = n_steps;
+    const size_t n = (size_t)d.n_particles;
+    r->pos.assign(d.position, d.position + 3 * n);
+    if (d.velocity) r->vel.assign(d.velocity, d.velocity + 3 * n);
+    r->mass.resize(n);
+    for (size_t q = 0; q < n; ++q) r->mass[q] = d.mass ? d.mass[q] : 1.0f;
+    r->bytes = estimate_bytes(d);
+    r->desc.position = nullptr;
+    r->desc.velocity = nullptr;
+    r->desc.mass = nullptr;
+    if (r->bytes > s->cfg.hbm_budget_bytes) {
+        set_last_error("scene footprint exceeds the server's HBM budget");
+        return BM_ERR_OUT_OF_MEMORY;
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        r->t_submit = Clock::now();
+        s->all[r->id] = r;
+        s->queue.push_back(r);
+        ++s->submitted;
+    }
+    s->cv_work.notify_all();
+    *request_id = r->id;
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_poll(bm_server_t* s, int64_t id, int32_t* state) {
+    if (!s || !state) return invalid_arg("NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return BM_ERR_NOT_FOUND;
+    *state = it->second->state;
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_wait(bm_server_t* s, int64_t id, int32_t timeout_ms) {
+    if (!s) return invalid_arg("NULL handle");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return BM_ERR_NOT_FOUND;
+    auto r = it->second;
+    const bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(std::max(0, timeout_ms)), [&] {
+        return r->state == BM_REQ_DONE || r->state == BM_REQ_FAILED || r->state == BM_REQ_CANCELLED;
+    });
+    if (!ok) {
+        set_last_error("request not finished within the timeout");
+        return BM_ERR_TIMEOUT;
+    }
+    if (r->state == BM_REQ_FAILED) return r->error != BM_OK ? r->error : BM_ERR_CUDA;
+    if (r->state == BM_REQ_CANCELLED) return BM_ERR_STATE;
+    return r->error;
+}
+
+BM_API bm_status_t bm_server_result(bm_server_t* s, int64_t id, const bm_particles_view_t* v, bm_collider_t* body,
+                                    double* latency_ms) {
+    if (!s) return invalid_arg("NULL handle");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return BM_ERR_NOT_FOUND;
+    Request& r = *it->second;
+    if (r.state != BM_REQ_DONE) {
+        set_last_error("request has no result");
+        return BM_ERR_STATE;
+    }
+    const size_t n = r.mass.size();
+    if (v) {
+        if (v->position) std::memcpy(v->position, r.out_pos.data(), sizeof(float) * 3 * n);
+        if (v->velocity) std::memcpy(v->velocity, r.out_vel.data(), sizeof(float) * 3 * n);
+        if (v->F) std::memcpy(v->F, r.out_F.data(), sizeof(float) * 9 * n);
+        if (v->C) std::memcpy(v->C, r.out_C.data(), sizeof(float) * 9 * n);
+        if (v->mass) std::memcpy(v->mass, r.mass.data(), sizeof(float) * n);
+    }
+    if (body) *body = r.out_body;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_release(bm_server_t* s, int64_t id) {
+    if (!s) return invalid_arg("NULL handle");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return BM_ERR_NOT_FOUND;
+    if (it->second->state == BM_REQ_QUEUED || it->second->state == BM_REQ_RUNNING) return BM_ERR_STATE;
+    s->all.erase(it);
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_cancel(bm_server_t* s, int64_t id) {
+    if (!s) return invalid_arg("NULL handle");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return BM_ERR_NOT_FOUND;
+    it->second->cancel = true;
+    s->cv_work.notify_all();
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_server_stats(bm_server_t* s, bm_server_stats_t* out) {
+    if (!s || !out) return invalid_arg("NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    bm_server_stats_t r{};
+    r.submitted = s->submitted;
+    r.completed = s->completed;
+    r.failed = s->failed;
+    r.cancelled = s->cancelled;
+    r.queued = (int64_t)s->queue.size();
+    r.active = s->n_active;
+    r.iterations = s->iterations;
+    r.p50_latency_ms = percentile(s->latencies, 0.50);
+    r.p99_latency_ms = percentile(s->latencies, 0.99);
+    double sum = 0;
+    for (double x : s->latencies) sum += x;
+    r.mean_latency_ms = s->latencies.empty() ? 0.0 : sum / (double)s->latencies.size();
+    r.particle_steps = s->particle_steps;
+    r.busy_seconds = s->busy;
+    r.peak_bytes = s->peak_bytes;
+    *out = r;
+    return BM_OK;
+}
+
+}  // extern "C"

@@ -124,6 +124,19 @@ void World::release() {
     stream = nullptr;
 }
 
+void World::remove_scene(int index) {
+    if (index < 0 || index >= (int)scenes.size()) return;
+    cudaStreamSynchronize(stream);
+    free_scene(scenes[index]);
+    scenes.erase(scenes.begin() + index);
+    dirty = true;
+}
+
+bm_status_t World::p2g_fresh() {
+    timed("p2g", [&] { launch_p2g(table(), n_ctas(), cur, sel, stream, true); });
+    return launch_status("p2g_fresh");
+}
+
 int World::add_scene() {
     scenes.emplace_back();
     SceneHost& h = scenes.back();

@@ -87,6 +87,10 @@ public:
     bm_status_t append_particles(SceneHost& h, int64_t n, const float* pos, const float* vel, const float* mass);
     void update_bbox(SceneHost& h, int64_t n, const float* pos);
     void free_scene(SceneHost& h);
+    void remove_scene(int index);
+    // P2G into acc[cur] of the scenes flagged `fresh` (their accumulators
+    // are still zero), leaving the other scenes' precomputed P2G alone.
+    bm_status_t p2g_fresh();
 
     // Device table.
     bm_status_t sync_table();

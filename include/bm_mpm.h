@@ -278,6 +278,59 @@ BM_API bm_status_t bm_batch_autotune(bm_batch_t* b, int32_t trial_steps, bm_tune
 BM_API bm_status_t bm_batch_timer_start(bm_batch_t* b);
 BM_API bm_status_t bm_batch_timer_stop(bm_batch_t* b, double* ms);
 
+/* ---- serving loop: continuous batching ---------------------------------
+ * No reference counterpart. A server owns one GPU stream and a worker
+ * thread. Requests (a scene and a number of steps) are queued by
+ * bm_server_submit from any thread; at every step boundary the worker admits
+ * queued requests in order while their estimated device footprint fits the
+ * HBM budget, steps all co-resident scenes together (one launch per phase
+ * for all of them, so their work overlaps on the device), and retires the
+ * scenes that have done their steps, copying their particles and body back
+ * to host memory. Waits are bounded (bm_server_wait returns BM_ERR_TIMEOUT). */
+typedef struct bm_server bm_server_t;
+
+typedef struct bm_server_config {
+    double hbm_budget_bytes;  /* admission budget, default 150e9 */
+    int32_t max_active;       /* most co-resident scenes, default 1024 */
+    int32_t sort_interval;    /* steps between regroupings, default 16 */
+    int32_t variant;          /* launch shape of the fused kernel, default 1 */
+} bm_server_config_t;
+
+typedef enum bm_request_state {
+    BM_REQ_QUEUED = 0,
+    BM_REQ_RUNNING = 1,
+    BM_REQ_DONE = 2,
+    BM_REQ_FAILED = 3,
+    BM_REQ_CANCELLED = 4
+} bm_request_state_t;
+
+typedef struct bm_server_stats {
+    int64_t submitted, completed, failed, cancelled, queued, active;
+    int64_t iterations;        /* batched steps launched */
+    double p50_latency_ms, p99_latency_ms, mean_latency_ms;  /* submit -> result ready */
+    double particle_steps;     /* of completed requests */
+    double busy_seconds;       /* wall time with scenes on the device */
+    double peak_bytes;         /* largest admitted footprint */
+} bm_server_stats_t;
+
+BM_API bm_status_t bm_server_create(const bm_server_config_t* config, bm_server_t** out);
+/* Stops the worker; queued and running requests are cancelled. */
+BM_API bm_status_t bm_server_destroy(bm_server_t* s);
+/* Copies the scene's arrays; the caller may free them on return. */
+BM_API bm_status_t bm_server_submit(bm_server_t* s, const bm_scene_desc_t* scene, int32_t n_steps,
+                                    int64_t* request_id);
+BM_API bm_status_t bm_server_poll(bm_server_t* s, int64_t request_id, int32_t* state);
+/* Waits at most timeout_ms for the request to finish. */
+BM_API bm_status_t bm_server_wait(bm_server_t* s, int64_t request_id, int32_t timeout_ms);
+/* Final particles (add order) and body of a finished request; any pointer may be NULL. */
+BM_API bm_status_t bm_server_result(bm_server_t* s, int64_t request_id, const bm_particles_view_t* view,
+                                    bm_collider_t* body, double* latency_ms);
+BM_API bm_status_t bm_server_release(bm_server_t* s, int64_t request_id);
+BM_API bm_status_t bm_server_cancel(bm_server_t* s, int64_t request_id);
+BM_API bm_status_t bm_server_stats(bm_server_t* s, bm_server_stats_t* out);
+/* Device bytes the admission policy charges for a scene. */
+BM_API bm_status_t bm_server_estimate_bytes(const bm_scene_desc_t* scene, double* bytes);
+
 #ifdef __cplusplus
 }
 #endif

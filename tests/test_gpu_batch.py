@@ -57,6 +57,11 @@ def test_batch_of_one_equals_plain_solver():
 
 
 def test_graph_replay_equals_eager_steps():
+    """Graph replay takes exactly the eager step sequence. FP32 atomics add in
+    a different order on every run, and in a contact scene that difference
+    grows with the steps (two eager runs of these scenes already differ by
+    ~2e-5 dx at 50 steps), so the bar is the accuracy bar; a step missed or
+    taken twice moves the falling sand by ~1e-2 dx."""
     scs = small_scenes(4)
     runs = []
     for graph in (True, False):
@@ -66,7 +71,7 @@ def test_graph_replay_equals_eager_steps():
         assert b.steps_done() == 53
         runs.append([b.get_particles(i)["position"] for i in range(len(scs))])
     for i, sc in enumerate(scs):
-        assert max_err_dx(runs[0][i], runs[1][i], sc.dx) < 1e-5
+        assert max_err_dx(runs[0][i], runs[1][i], sc.dx) < POS_TOL_100
 
 
 def test_autotune_leaves_the_scenes_where_they_were():
@@ -80,7 +85,8 @@ def test_autotune_leaves_the_scenes_where_they_were():
     b = bm.Batch(scs)
     b.step(25)
     for i, sc in enumerate(scs):
-        assert max_err_dx(a.get_particles(i)["position"], b.get_particles(i)["position"], sc.dx) < 1e-5
+        # atomic-order bound of a contact scene, as in the graph test above
+        assert max_err_dx(a.get_particles(i)["position"], b.get_particles(i)["position"], sc.dx) < POS_TOL_100
 
 
 def test_batch_reports_the_failing_scene():
