@@ -163,6 +163,7 @@ _SIGS = {
     "bm_batch_autotune": (_st, [_h, C.c_int32, C.POINTER(TuneResult)]),
     "bm_batch_timer_start": (_st, [_h]),
     "bm_batch_timer_stop": (_st, [_h, C.POINTER(C.c_double)]),
+    "bm_coupler_m1_apply_noalloc": (_st, [_h, C.c_int32, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
     "bm_server_create": (_st, [C.POINTER(ServerConfig), C.POINTER(_h)]),
     "bm_server_destroy": (_st, [_h]),
     "bm_server_submit": (_st, [_h, C.POINTER(SceneDesc), C.c_int32, C.POINTER(C.c_int64)]),

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -691,3 +692,106 @@ BM_API int32_t bm_launch_variant_count(void) { return fused_variant_count(); }
 BM_API const char* bm_launch_variant_name(int32_t variant) { return fused_variant_name(variant); }
 
 }  // extern "C"
+
+// ---- M1 coupler without allocation ----------------------------------------
+//
+// bm_coupler_m1_apply_noalloc runs the M1 kernels of bm_coupler_m1_apply, but
+// its scratch comes from one fixed array in this file, not from the
+// per-solver buffers that the other coupler calls grow with cudaMalloc on first
+// use. The scratch holds the per-body FP64 reaction sums, the per-body
+// parameter blocks and the finished reactions, for at most kNoAllocMaxBodies
+// bodies. Some hosts call the coupler where a device allocation is not
+// allowed. One is a fixed-budget simulation tick: cudaMalloc and cudaFree can
+// wait for the whole device. Another is a process whose HBM is already held
+// by a memory pool, where even a small cudaMalloc fails. Such hosts call this
+// entry point instead.
+//
+// The array is shared by every solver on a device. Two calls that overlap in
+// time (from two host threads, on any streams) race on it and give wrong
+// reactions; callers must serialise them. The first call on each device looks
+// up the array's device address (cudaGetSymbolAddress) and keeps it; make that
+// first call before any stream capture begins on that device.
+
+namespace {
+
+constexpr int kNoAllocMaxBodies = 64;
+constexpr int kNoAllocMaxDevices = 64;
+
+constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kNoAllocAccOff = 0;  // double[7] per body: force, torque, nodes_inside
+constexpr size_t kNoAllocParamOff = kNoAllocAccOff + align256(sizeof(double) * 7 * kNoAllocMaxBodies);
+constexpr size_t kNoAllocReactOff = kNoAllocParamOff + align256(sizeof(M1Params) * kNoAllocMaxBodies);
+constexpr size_t kNoAllocBytes = kNoAllocReactOff + align256(sizeof(bm_reaction_t) * kNoAllocMaxBodies);
+static_assert(alignof(M1Params) <= 256 && alignof(bm_reaction_t) <= 256, "scratch regions start on 256 B");
+static_assert(kNoAllocBytes <= 32 * 1024, "the fixed scratch stays modest");
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_m1_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on `dev` (the current device), looked up
+// once per device.
+bm_status_t noalloc_scratch(int dev, unsigned char** out) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return invalid_arg("device index beyond the no-alloc scratch table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_m1_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_last_error(std::string("cudaGetSymbolAddress(no-alloc M1 scratch): ") + cudaGetErrorString(e));
+            return BM_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return BM_OK;
+}
+
+}  // namespace
+
+BM_API bm_status_t bm_coupler_m1_apply_noalloc(bm_solver_t* s, int32_t n_bodies, const bm_collider_t* bodies,
+                                               float dt, bm_reaction_t* out) {
+    if (!s) return invalid_arg("NULL handle");
+    if (n_bodies < 0 || (n_bodies > 0 && (!bodies || !out))) return invalid_arg("bad bodies or reactions");
+    if (n_bodies > kNoAllocMaxBodies)
+        return invalid_arg("bm_coupler_m1_apply_noalloc takes at most 64 bodies per call (fixed scratch)");
+    DeviceGuard dg(s->w.device);
+    if (n_bodies > 0) std::memset(out, 0, sizeof(bm_reaction_t) * n_bodies);
+    // The grid and the scene table must already exist: building them allocates.
+    if (!s->sc().grid_ready || s->w.dirty || (!s->acc_valid && s->sc().n() > 0)) {
+        set_last_error("bm_coupler_m1_apply_noalloc needs the grid of bm_solver_p2g and bm_solver_grid_update");
+        return BM_ERR_STATE;
+    }
+    if (n_bodies == 0) return BM_OK;
+    unsigned char* base = nullptr;
+    bm_status_t st = noalloc_scratch(s->w.device, &base);
+    if (st != BM_OK) return st;
+    double* acc = reinterpret_cast<double*>(base + kNoAllocAccOff);
+    M1Params* params = reinterpret_cast<M1Params*>(base + kNoAllocParamOff);
+    bm_reaction_t* react = reinterpret_cast<bm_reaction_t*>(base + kNoAllocReactOff);
+
+    M1Params hp[kNoAllocMaxBodies];
+    for (int b = 0; b < n_bodies; ++b) m1_prepare(s->sc().dev.g, bodies[b], dt, 0, &hp[b]);
+    cudaStream_t stream = s->w.stream;
+    // the reaction sums start at zero on every call
+    BM_CHECK_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 7 * n_bodies, stream));
+    BM_CHECK_CUDA(cudaMemcpyAsync(params, hp, sizeof(M1Params) * n_bodies, cudaMemcpyHostToDevice, stream));
+    // one launch per body, in order: a body sees the grid its predecessors
+    // projected, as the reference's couplers applied one after another do
+    for (int b = 0; b < n_bodies; ++b)
+        if (hp[b].active)
+            launch_m1(s->w.table(), params + b, 1, (int64_t)hp[b].nbi * hp[b].nbj * hp[b].nbk, s->w.cur,
+                      acc + 7 * b, stream);
+    launch_reaction_finalize(acc, n_bodies, react, stream);
+    s->view = s->w.cur;
+    st = launch_status("m1 (no-alloc)");
+    if (st != BM_OK) return st;
+    BM_CHECK_CUDA(cudaMemcpyAsync(out, react, sizeof(bm_reaction_t) * n_bodies, cudaMemcpyDeviceToHost, stream));
+    BM_CHECK_CUDA(cudaStreamSynchronize(stream));
+    return BM_OK;
+}

@@ -164,6 +164,19 @@ BM_API bm_status_t bm_solver_grid_update(bm_solver_t* s, float dt);
  * leaves the grid unchanged. `out` is written before the call returns. */
 BM_API bm_status_t bm_coupler_m1_apply(bm_solver_t* s, const bm_collider_t* body, float dt,
                                        bm_reaction_t* out);
+/* No counterpart in the reference. The M1 apply above for up to 64 bodies
+ * that allocates nothing: its scratch is a fixed 256-byte-aligned device array
+ * of about 15 KB in the library, not buffers grown with cudaMalloc. For hosts
+ * that may not allocate device memory at the call site: a fixed-budget tick
+ * (cudaMalloc/cudaFree can wait for the whole device), or a process whose HBM
+ * a pool already holds. n_bodies > 64 gives BM_ERR_INVALID_ARGUMENT; calling it
+ * before bm_solver_p2g + bm_solver_grid_update have built the grid gives
+ * BM_ERR_STATE. The array is shared by all solvers on a device: calls that
+ * overlap in time race on it, so serialise them. The first call on a device
+ * looks up the array's address; make it before any stream capture begins.
+ * `out` (n_bodies entries) is written before the call returns. */
+BM_API bm_status_t bm_coupler_m1_apply_noalloc(bm_solver_t* s, int32_t n_bodies, const bm_collider_t* bodies,
+                                               float dt, bm_reaction_t* out);
 /* The G2P loop (:83-86). */
 BM_API bm_status_t bm_solver_g2p(bm_solver_t* s, float dt);
 /* P2G, grid update, M1 for each body in order, G2P, all on the handle's
