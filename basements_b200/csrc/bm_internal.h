@@ -242,6 +242,12 @@ struct M1Params {
     int bi0, bj0, bk0, nbi, nbj, nbk;  // candidate block range (relative to box)
 };
 bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* out);
+// True when the candidate block ranges of two bodies of one scene intersect
+// (they may then write the same nodes).
+inline bool m1_blocks_overlap(const M1Params& a, const M1Params& b) {
+    return a.bi0 < b.bi0 + b.nbi && b.bi0 < a.bi0 + a.nbi && a.bj0 < b.bj0 + b.nbj && b.bj0 < a.bj0 + a.nbj &&
+           a.bk0 < b.bk0 + b.nbk && b.bk0 < a.bk0 + a.nbk;
+}
 // Candidate blocks the AABB of a body with these half extents can span.
 int64_t m1_max_candidates(const GridDesc& g, const float half_extents[3]);
 // One CTA of 64 threads per candidate block: grid (max_candidates, n_bodies).

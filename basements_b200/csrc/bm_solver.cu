@@ -121,18 +121,38 @@ bm_status_t do_m1(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float
     bm_status_t st = ensure_reactions(s, std::max(1, n_bodies));
     if (st != BM_OK) return st;
     s->h_params.resize(n_bodies);
-    int64_t max_cand = 0;
+    std::vector<M1Params>& hp = s->h_params;
+    bool any_active = false;
     for (int b = 0; b < n_bodies; ++b) {
-        m1_prepare(s->sc().dev.g, bodies[b], dt, 0, &s->h_params[b]);
-        const M1Params& P = s->h_params[b];
-        if (P.active) max_cand = std::max<int64_t>(max_cand, (int64_t)P.nbi * P.nbj * P.nbk);
+        m1_prepare(s->sc().dev.g, bodies[b], dt, 0, &hp[b]);
+        any_active = any_active || hp[b].active;
     }
     BM_CHECK_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(double) * 7 * n_bodies, s->w.stream));
-    if (n_bodies > 0 && max_cand > 0) {
-        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_params, s->h_params.data(), sizeof(M1Params) * n_bodies,
-                                      cudaMemcpyHostToDevice, s->w.stream));
+    if (any_active) {
+        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_params, hp.data(), sizeof(M1Params) * n_bodies, cudaMemcpyHostToDevice,
+                                      s->w.stream));
+        // The reference applies its couplers one after another, each on the
+        // grid its predecessor left. Bodies whose candidate blocks are
+        // disjoint touch disjoint nodes and share one launch; a body that
+        // overlaps an earlier body of the current launch starts the next one.
         s->w.timed("m1_coupler", [&] {
-            launch_m1(s->w.table(), s->d_params, n_bodies, max_cand, s->w.cur, s->d_acc, s->w.stream);
+            int first = 0;
+            while (first < n_bodies) {
+                int last = first;
+                int64_t cand = 0;
+                for (; last < n_bodies; ++last) {
+                    const M1Params& P = hp[last];
+                    if (!P.active) continue;
+                    bool clash = false;
+                    for (int q = first; q < last && !clash; ++q) clash = hp[q].active && m1_blocks_overlap(hp[q], P);
+                    if (clash) break;
+                    cand = std::max<int64_t>(cand, (int64_t)P.nbi * P.nbj * P.nbk);
+                }
+                if (cand > 0)
+                    launch_m1(s->w.table(), s->d_params + first, last - first, cand, s->w.cur, s->d_acc + 7 * first,
+                              s->w.stream);
+                first = last;
+            }
         });
     }
     launch_reaction_finalize(s->d_acc, n_bodies, s->d_react, s->w.stream);

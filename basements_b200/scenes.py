@@ -131,6 +131,28 @@ def scaled_wheel_rut(n_keep: int, seed=1) -> Scene:
     return wheel_rut(n_keep=n_keep, seed=seed)
 
 
+def _sand_block(rng, G: int, N: int, ppc: int = 8):
+    """A block of w x h x w cells at `ppc` jittered particles per cell, centred
+    in x/z on the floor, h ~ w/2; the first N particles of it."""
+    dx = 1.0 / G
+    cells = max(1, N // ppc)
+    w = max(2, min(G - 8, int(round((cells / 0.5) ** (1.0 / 3.0)))))
+    h = max(1, int(math.ceil(cells / (w * w))))
+    ncell = w * w * h
+    pos = np.empty((ncell * ppc, 3), np.float32)
+    ii, jj, kk = np.meshgrid(np.arange(w), np.arange(h), np.arange(w), indexing="ij")
+    base = np.stack([ii + (G - w) // 2, jj, kk + (G - w) // 2], -1).reshape(-1, 3).astype(np.float32)
+    jit = rng.random((ncell, ppc, 3), dtype=np.float32)
+    pos[:] = ((base[:, None, :] + jit) * np.float32(dx)).reshape(-1, 3)
+    return pos[:N], h
+
+
+def _stable_dt(E, nu, rho, dx):
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    return min(2e-4, 0.5 * dx / math.sqrt((lam + 2 * mu) / rho))
+
+
 def box_drop_scene(seed: int, grid: int | None = None, n_particles: int | None = None) -> Scene:
     """One uneven batched scene: grid side in {32,48,64,96}, particle count
     log-uniform 8k-400k at 8 ppc, friction angle U[25,40] deg, E log-uniform
@@ -141,17 +163,7 @@ def box_drop_scene(seed: int, grid: int | None = None, n_particles: int | None =
     N = n_particles or int(math.exp(rng.uniform(math.log(8e3), math.log(4e5))))
     dx = 1.0 / G
     ppc = 8
-    cells = max(1, N // ppc)
-    # a sand block centred in x/z resting on the floor: width w x height h x w cells
-    w = max(2, min(G - 8, int(round((cells / 0.5) ** (1.0 / 3.0)))))
-    h = max(1, int(math.ceil(cells / (w * w))))
-    ncell = w * w * h
-    pos = np.empty((ncell * ppc, 3), np.float32)
-    ii, jj, kk = np.meshgrid(np.arange(w), np.arange(h), np.arange(w), indexing="ij")
-    base = np.stack([ii + (G - w) // 2, jj, kk + (G - w) // 2], -1).reshape(-1, 3).astype(np.float32)
-    jit = rng.random((ncell, ppc, 3), dtype=np.float32)
-    pos[:] = ((base[:, None, :] + jit) * np.float32(dx)).reshape(-1, 3)
-    pos = pos[:N]
+    pos, h = _sand_block(rng, G, N, ppc)
     rho = 1600.0
     E = float(math.exp(rng.uniform(math.log(1e5), math.log(1e6))))
     phi = float(rng.uniform(25.0, 40.0))
@@ -163,10 +175,44 @@ def box_drop_scene(seed: int, grid: int | None = None, n_particles: int | None =
                 linear_velocity=(0.0, -float(rng.uniform(0.0, 1.0)), 0.0), mass=float(rho * side ** 3),
                 shape=0, kinematic=False)
     nu = 0.3
-    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
-    mu = E / (2 * (1 + nu))
-    c = math.sqrt((lam + 2 * mu) / rho)
-    dt = min(2e-4, 0.5 * dx / c)
+    dt = _stable_dt(E, nu, rho, dx)
     m = np.float32(rho * dx ** 3 / ppc)
     return Scene(f"box_drop_{seed}", dx, G, pos, np.full(len(pos), m, np.float32), E, nu, rho, dp_alpha(phi),
                  dt, 500, bodies=[body])
+
+
+def serve_request_scene(seed: int) -> Scene:
+    """One request of the serving stream: grid side uniform in [32, 128],
+    particle count log-uniform in [10k, 1M] (capped at 8 ppc over a quarter of
+    the G^3 box, so that the bed fits its grid), 100-2000 steps, friction angle
+    U[25, 40] deg on the sand-column material (E = 3.5e5 Pa, nu = 0.3,
+    rho = 1600 kg/m^3). With probability 1/2 a dynamic rigid body, a box or a
+    cylinder with equal probability (side / diameter U[0.05, 0.2] m, random
+    pose, dropped at U[0, 1] m/s), falls on the bed. The grid box spans G/2
+    cells beyond the bed on each side in x and z, so that the runout of the
+    sand stays inside it."""
+    rng = np.random.default_rng(500_000 + seed)
+    G = int(rng.integers(32, 129))
+    n_cap = int(8 * 0.25 * G ** 3)
+    N = min(n_cap, int(math.exp(rng.uniform(math.log(1e4), math.log(1e6)))))
+    steps = int(rng.integers(100, 2001))
+    dx = 1.0 / G
+    pos, h = _sand_block(rng, G, N, 8)
+    rho, E, nu = 1600.0, 3.5e5, 0.3
+    phi = float(rng.uniform(25.0, 40.0))
+    bodies = []
+    if rng.random() < 0.5:
+        shape = int(rng.random() < 0.5)
+        side = float(rng.uniform(0.05, 0.2))
+        q = rng.normal(size=4)
+        q = q / np.linalg.norm(q)
+        he = (side / 2, side / 2, side / 2)
+        mass = rho * side ** 3 if shape == 0 else rho * math.pi * (side / 2) ** 2 * side
+        bodies.append(Body(center=(0.5, (h + 2) * dx + side, 0.5), half_extents=he,
+                           orientation=tuple(map(float, q)),
+                           linear_velocity=(0.0, -float(rng.uniform(0.0, 1.0)), 0.0), mass=float(mass),
+                           shape=shape, kinematic=False))
+    m = np.float32(rho * dx ** 3 / 8)
+    dom = ((-G // 2, -4, -G // 2), (2 * G, G + 8, 2 * G))
+    return Scene(f"request_{seed}", dx, G, pos, np.full(len(pos), m, np.float32), E, nu, rho, dp_alpha(phi),
+                 _stable_dt(E, nu, rho, dx), steps, bodies=bodies, domain=dom)

@@ -7,6 +7,13 @@ Workload (default): the plain large rigid-wheel rut, 2,000,000 particles on a
 M1 coupler, G2P. Synthetic seeded inputs (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--forms plain,batched,served]
+
+Beside the headline plain step the line carries the two other forms of the
+metric (one GPU only): "batched" (256 uneven box-drop scenes stepped
+together) and "served" (Poisson request streams into the continuous-batching
+server, with p50/p99 latency), each with the plain per-scene loop on the same
+scenes and the ratio to it.
 
 N > 1 runs N independent replicas (one per GPU, launched by torchrun); the
 path has no inter-GPU exchange, so there is no collective on the data path.
@@ -46,6 +53,12 @@ def parse():
                     help="SVD arithmetic of the fused step (default: the library default)")
     ap.add_argument("--sort-interval", type=int, default=None)
     ap.add_argument("--variant", type=int, default=None, help="launch shape of the fused kernel")
+    ap.add_argument("--forms", default="plain,batched,served",
+                    help="comma list: plain (the headline wheel rut), batched (256 uneven scenes), "
+                         "served (Poisson request stream)")
+    ap.add_argument("--batch-scenes", type=int, default=256)
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-rates", default="200,10", help="arrival rates (req/s) of the served runs")
     return ap.parse_args()
 
 
@@ -290,6 +303,167 @@ def run_e2e(args, sc, ranks: Ranks):
             "what": "upload + K synchronous coupled steps (host collider in, host reaction out) + download"}
 
 
+def _host_body_step(body: dict, force, torque, gravity, dt):
+    """The reference TimeIntegrator step (integrator.h:19-57) on a host body,
+    with the identity body-space inverse inertia the reference scenarios leave
+    in place: v += (m g + F)/m dt, w += tau dt, x += v dt, q += dt/2 (0,w) q."""
+    m = body["mass"]
+    v = [body["linear_velocity"][i] + (gravity[i] * m + float(force[i])) / m * dt for i in range(3)]
+    w = [body["angular_velocity"][i] + float(torque[i]) * dt for i in range(3)]
+    body["linear_velocity"], body["angular_velocity"] = tuple(v), tuple(w)
+    body["center"] = tuple(body["center"][i] + v[i] * dt for i in range(3))
+    qw, qx, qy, qz = body["orientation"]
+    wx, wy, wz = w
+    dq = (-wx * qx - wy * qy - wz * qz, wx * qw + wy * qz - wz * qy, -wx * qz + wy * qw + wz * qx,
+          wx * qy - wy * qx + wz * qw)
+    q = [body["orientation"][k] + 0.5 * dt * dq[k] for k in range(4)]
+    n = sum(c * c for c in q) ** 0.5
+    body["orientation"] = tuple(c / n for c in q) if n >= 1e-6 else (1.0, 0.0, 0.0, 0.0)
+
+
+def plain_scene_loop(scs, steps: int, warmup: int = 3):
+    """The plain per-scene loop: the scenes one after another through the
+    drop-in solver API, each stepped `steps` times after `warmup` untimed
+    steps. A dynamic body takes the reaction back to the host every step and
+    is integrated there, as the reference's coupling harness does
+    (bench_compare_all.cpp:104-116). Host-clock time, synchronised at both
+    ends of each scene's timed steps (the loop's host round trips are part of
+    what it costs). Returns (particle-steps/s, particle-steps, seconds)."""
+    import basements_b200 as bm
+
+    work, secs = 0, 0.0
+    for sc in scs:
+        s = bm.MPMSolver(sc.dx, domain=sc.domain)
+        s.set_material(sc.E, sc.nu, sc.rho)
+        s.set_plastic_alpha(sc.alpha)
+        s.set_floor_friction(sc.floor_friction)
+        s.set_gravity(sc.gravity)
+        s.add_particles(sc.position, None, sc.mass)
+        body = dict(sc.bodies[0].as_tuple()) if sc.bodies else None
+
+        def one():
+            if body is None:
+                s.step(sc.dt)
+            else:
+                f, t, _ = s.step_coupled(sc.dt, [bm.make_collider(**body)])[0]
+                _host_body_step(body, f, t, sc.gravity, sc.dt)
+
+        for _ in range(warmup):
+            one()
+        s.sync()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            one()
+        st, _ = s.sync()
+        secs += time.perf_counter() - t0
+        if st != 0:
+            raise RuntimeError(f"plain loop: scene {sc.name} reported status {st}")
+        work += sc.n * steps
+        s.close()
+    return work / secs, work, secs
+
+
+def run_batched(args):
+    """Batched form: 256 box-drop scenes of uneven size (grid side in
+    {32,48,64,96}, 8k-400k particles, dynamic boxes) in one batch: one
+    persistent launch per phase over the scene table, CUDA-graph chunks,
+    launch shape and sort interval chosen by the autotuner. K steps timed with
+    CUDA events on the batch stream, inputs resident (GBs, beyond L2)."""
+    import basements_b200 as bm
+    from basements_b200 import scenes
+
+    scs = [scenes.box_drop_scene(i) for i in range(args.batch_scenes)]
+    n_tot = sum(sc.n for sc in scs)
+    b = bm.Batch(scs)
+    b.step(1)
+    tune = b.autotune(trial_steps=16)
+    for _ in range(args.warmup):
+        b.step(1)
+    b.sync()
+    b.timer_start()
+    b.step(args.steps)
+    ms = b.timer_stop()
+    st, bad, esc = b.sync()
+    if st != 0:
+        raise RuntimeError(f"batched: scene {bad} reported status {st}")
+    b.close()
+    value = n_tot * args.steps / (ms / 1e3)
+    loop_steps = min(args.steps, 50)
+    loop_rate, loop_work, loop_secs = plain_scene_loop(scs, loop_steps)
+    return {"workload": f"{len(scs)} box-drop scenes, grid side in {{32,48,64,96}}, 8k-400k particles "
+                        "(log-uniform, 8 ppc), friction angle 25-40 deg, E 1e5-1e6 Pa, dynamic M1 box",
+            "scenes": len(scs), "particles": n_tot, "value": value, "unit": UNIT, "steps": args.steps,
+            "ms_per_step": ms / args.steps, "timing": "CUDA events on the batch stream",
+            "autotune": tune,
+            "plain_loop": {"value": loop_rate, "unit": UNIT, "steps_per_scene": loop_steps,
+                           "seconds": loop_secs,
+                           "what": "same scenes one after another through bm_solver_step_coupled, reaction "
+                                   "read back and the body integrated on the host every step (host clock)"},
+            "speedup_vs_plain_loop": value / loop_rate}
+
+
+def run_served(args):
+    """Served form: Poisson request streams into the continuous-batching
+    server (bm_server_*), one per arrival rate; each request is a seeded
+    scene of 10k-1M particles on a 32-128 grid for 100-2000 steps, half with a
+    dynamic box or cylinder. Reported per rate: throughput = particle-steps of
+    all requests / (last completion - first arrival), host clock, and the
+    server's p50/p99 submit-to-result latency. The plain per-request loop runs
+    the same requests one after another through the drop-in solver API."""
+    import basements_b200 as bm
+    from basements_b200 import scenes
+
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
+    runs = []
+    base_seed = 0
+    all_reqs = []
+    for ri, rate in enumerate(rates):
+        reqs = [scenes.serve_request_scene(base_seed + i) for i in range(args.serve_requests)]
+        base_seed += args.serve_requests
+        all_reqs += reqs
+        rng = np.random.default_rng(77 + ri)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+        arrivals -= arrivals[0]
+        srv = bm.Server()
+        w = srv.submit(scenes.serve_request_scene(10_000_000), 20)  # context and kernels warm
+        if srv.wait(w) != 0:
+            raise RuntimeError("served: warm-up request failed")
+        srv.release(w)
+        work = sum(sc.n * sc.steps for sc in reqs)
+        ids = []
+        t0 = time.perf_counter()
+        for sc, at in zip(reqs, arrivals):
+            d = t0 + at - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(sc, sc.steps))
+        for r in ids:
+            if srv.wait(r, timeout_ms=600_000) != 0:
+                raise RuntimeError(f"served: request {r} did not complete")
+        el = time.perf_counter() - t0
+        lat = [srv.result(r)["latency_ms"] for r in ids]
+        st = srv.stats()
+        srv.close()
+        runs.append({"rate_req_s": rate, "requests": len(reqs), "particle_steps": work,
+                     "value": work / el, "unit": UNIT, "seconds": el,
+                     "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
+                     "server_p50_ms": st["p50_latency_ms"], "server_p99_ms": st["p99_latency_ms"],
+                     "gpu_busy_rate": st["particle_steps"] / max(st["busy_seconds"], 1e-9),
+                     "iterations": st["iterations"], "peak_bytes": st["peak_bytes"]})
+    loop_steps = 100
+    loop_rate, _, loop_secs = plain_scene_loop(all_reqs[:args.serve_requests], loop_steps)
+    best = max(r["value"] for r in runs)
+    return {"workload": "Poisson request stream: grid 32-128, 10k-1M particles (log-uniform, capped to fit "
+                        "the grid), 100-2000 steps, friction angle 25-40 deg, half with a dynamic box or "
+                        "cylinder; admission by a 150 GB HBM budget",
+            "runs": runs, "value": best, "unit": UNIT,
+            "plain_loop": {"value": loop_rate, "unit": UNIT, "steps_per_request": loop_steps,
+                           "seconds": loop_secs,
+                           "what": "the first rate's requests one after another through the drop-in solver "
+                                   "(host clock, body integrated on the host every step)"},
+            "speedup_vs_plain_loop": best / loop_rate}
+
+
 def cpu_reference_rate(sc, n_steps: int, kind: str):
     """Times the reference's own CPU MPMSolver (oracle/_ref, else the pinned
     float restatement) on the wheel-rut scene: P2G, update_grid, M1 apply,
@@ -346,7 +520,12 @@ def main():
             if ranks.rank == 0:
                 print(json.dumps(run_reference(args, ranks)), flush=True)
             return
+        forms = set(f for f in args.forms.split(",") if f)
         out = run_ours(args, ranks)
+        if ranks.world == 1 and "batched" in forms:
+            out["batched"] = run_batched(args)
+        if ranks.world == 1 and "served" in forms:
+            out["served"] = run_served(args)
         if ranks.rank == 0 and not args.no_cpu_baseline:
             from basements_b200 import scenes
             from oracle import oracle as O
