@@ -164,6 +164,12 @@ _SIGS = {
     "bm_batch_timer_start": (_st, [_h]),
     "bm_batch_timer_stop": (_st, [_h, C.POINTER(C.c_double)]),
     "bm_coupler_m1_apply_noalloc": (_st, [_h, C.c_int32, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
+    "bm_tape_create": (_st, [_h, C.c_int32, C.POINTER(_h)]),
+    "bm_tape_destroy": (_st, [_h]),
+    "bm_tape_forward": (_st, [_h, C.c_float, C.c_int32, C.POINTER(Collider), C.c_int32, _f]),
+    "bm_adjoint_backward": (_st, [_h, _f, _f, _f, _f, _f]),
+    "bm_adjoint_backward_state": (_st, [_h, C.POINTER(ParticlesView), _f, C.POINTER(ParticlesView)]),
+    "bm_tape_body_grad": (_st, [_h, C.c_int32, C.POINTER(C.c_double)]),
     "bm_server_create": (_st, [C.POINTER(ServerConfig), C.POINTER(_h)]),
     "bm_server_destroy": (_st, [_h]),
     "bm_server_submit": (_st, [_h, C.POINTER(SceneDesc), C.c_int32, C.POINTER(C.c_int64)]),
@@ -607,3 +613,89 @@ def estimate_bytes(scene) -> float:
     b = C.c_double()
     check(lib().bm_server_estimate_bytes(C.byref(d), C.byref(b)), "bm_server_estimate_bytes")
     return b.value
+
+
+class Tape:
+    """Differentiable run on a solver (bm_tape_* / bm_adjoint_backward)."""
+
+    def __init__(self, solver: MPMSolver, checkpoint_every: int = 20):
+        self.solver = solver
+        self._h = C.c_void_p()
+        check(lib().bm_tape_create(solver._h, int(checkpoint_every), C.byref(self._h)), "bm_tape_create")
+        self.n_steps = 0
+        self.n_wp = 0
+
+    def close(self):
+        if self._h:
+            lib().bm_tape_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, dt, n_steps, body: Collider | None = None, waypoints=None):
+        """n_steps split steps recorded for the reverse pass; the body (if
+        any) follows the piecewise-linear path through `waypoints`."""
+        wp = None
+        self.n_wp = 0
+        if body is not None:
+            wp = np.ascontiguousarray(waypoints, np.float32).reshape(-1, 3)
+            self.n_wp = len(wp)
+        check(lib().bm_tape_forward(self._h, float(dt), int(n_steps), C.byref(body) if body is not None else None,
+                                    self.n_wp, _fp(wp) if wp is not None else None), "bm_tape_forward")
+        self.n_steps = int(n_steps)
+
+    def backward(self, dL_dx, dL_dv=None, want_x0=False, want_v0=False):
+        """Returns a dict with dL_dwaypoints (when the run had a body) and,
+        on request, dL_dx0 / dL_dv0."""
+        n = self.solver.num_particles()
+        gx = np.ascontiguousarray(dL_dx, np.float32).reshape(n, 3)
+        gv = None if dL_dv is None else np.ascontiguousarray(dL_dv, np.float32).reshape(n, 3)
+        out = {}
+        wp = np.zeros((self.n_wp, 3), np.float32) if self.n_wp else None
+        x0 = np.zeros((n, 3), np.float32) if want_x0 else None
+        v0 = np.zeros((n, 3), np.float32) if want_v0 else None
+        check(lib().bm_adjoint_backward(self._h, _fp(gx), _fp(gv) if gv is not None else None,
+                                        _fp(wp) if wp is not None else None, _fp(x0) if x0 is not None else None,
+                                        _fp(v0) if v0 is not None else None), "bm_adjoint_backward")
+        if wp is not None:
+            out["dL_dwaypoints"] = wp
+        if x0 is not None:
+            out["dL_dx0"] = x0
+        if v0 is not None:
+            out["dL_dv0"] = v0
+        return out
+
+    def backward_state(self, dL: dict):
+        """Reverse pass for the whole state: dL maps any of position, velocity
+        (n x 3), F, C (n x 3 x 3) to the loss gradient at the final state.
+        Returns the gradient at the initial state for the four fields, plus
+        dL_dwaypoints when the run had a body."""
+        n = self.solver.num_particles()
+        shapes = {"position": (n, 3), "velocity": (n, 3), "F": (n, 3, 3), "C": (n, 3, 3)}
+        keep = {}
+        vin = ParticlesView()
+        for k, shp in shapes.items():
+            if k in dL:
+                keep[k] = np.ascontiguousarray(dL[k], np.float32).reshape(shp)
+                setattr(vin, k, _fp(keep[k]))
+        out = {k: np.zeros(shp, np.float32) for k, shp in shapes.items()}
+        vout = ParticlesView()
+        for k in shapes:
+            setattr(vout, k, _fp(out[k]))
+        wp = np.zeros((self.n_wp, 3), np.float32) if self.n_wp else None
+        check(lib().bm_adjoint_backward_state(self._h, C.byref(vin), _fp(wp) if wp is not None else None,
+                                              C.byref(vout)), "bm_adjoint_backward_state")
+        if wp is not None:
+            out["dL_dwaypoints"] = wp
+        return out
+
+    def body_grad(self):
+        """dL/d(body linear velocity), dL/d(body angular velocity) per step (n_steps x 6)."""
+        g = np.zeros((self.n_steps, 6), np.float64)
+        check(lib().bm_tape_body_grad(self._h, self.n_steps, g.ctypes.data_as(C.POINTER(C.c_double))),
+              "bm_tape_body_grad")
+        return g

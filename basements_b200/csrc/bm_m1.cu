@@ -17,43 +17,14 @@
 #include <cmath>
 
 #include "bm_internal.h"
+#include "bm_m1.cuh"
 #include "bm_math.cuh"
 
 namespace bm {
 
 namespace {
 
-// Round-to-nearest float arithmetic that is never contracted into FMA: the
-// intrinsics on the device, plain operators on the host (host code is built
-// with -ffp-contract=off).
-__host__ __device__ __forceinline__ float mul(float a, float b) {
-#ifdef __CUDA_ARCH__
-    return __fmul_rn(a, b);
-#else
-    return a * b;
-#endif
-}
-__host__ __device__ __forceinline__ float add(float a, float b) {
-#ifdef __CUDA_ARCH__
-    return __fadd_rn(a, b);
-#else
-    return a + b;
-#endif
-}
-__host__ __device__ __forceinline__ float sub(float a, float b) {
-#ifdef __CUDA_ARCH__
-    return __fsub_rn(a, b);
-#else
-    return a - b;
-#endif
-}
-__host__ __device__ __forceinline__ float dvd(float a, float b) {
-#ifdef __CUDA_ARCH__
-    return __fdiv_rn(a, b);
-#else
-    return a / b;
-#endif
-}
+using namespace rn;
 
 // mpm_rigid_coupler_pic.h:100-117 plus the candidate block range.
 __host__ __device__ bool m1_params(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* P) {
@@ -126,36 +97,11 @@ __global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params,
     double f0 = 0, f1 = 0, f2 = 0, t0 = 0, t1 = 0, t2 = 0, cnt = 0;
     const int ox = g.ox + 4 * bi, oy = g.oy + 4 * bj, oz = g.oz + 4 * bk;
     const float dx = g.dx;
-    bool visit = S.alloc[blin] != 0;
-    if (visit) {
-        const float blo0 = mul((float)ox + 0.5f, dx), bhi0 = mul((float)(ox + 3) + 0.5f, dx);
-        const float blo1 = mul((float)oy + 0.5f, dx), bhi1 = mul((float)(oy + 3) + 0.5f, dx);
-        const float blo2 = mul((float)oz + 0.5f, dx), bhi2 = mul((float)(oz + 3) + 0.5f, dx);
-        if (bhi0 < P.lo[0] || blo0 > P.hi[0]) visit = false;
-        if (bhi1 < P.lo[1] || blo1 > P.hi[1]) visit = false;
-        if (bhi2 < P.lo[2] || blo2 > P.hi[2]) visit = false;
-    }
-    if (visit) {
+    if (m1_block_visited(P, g, S.alloc, bi, bj, bk)) {
         const int li = tt >> 4, lj = (tt >> 2) & 3, lk = tt & 3;
         const int64_t id = g.node_of_block(blin, tt);
-        const float xn[3] = {mul((float)(ox + li) + 0.5f, dx), mul((float)(oy + lj) + 0.5f, dx),
-                             mul((float)(oz + lk) + 0.5f, dx)};
-        const float r[3] = {sub(xn[0], P.c[0]), sub(xn[1], P.c[1]), sub(xn[2], P.c[2])};
-        float l[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-            l[a] = add(add(mul(P.R[a], r[0]), mul(P.R[3 + a], r[1])), mul(P.R[6 + a], r[2]));
-        bool inside;
-        if (P.shape == 1) {
-            const float r2 = add(mul(l[0], l[0]), mul(l[2], l[2]));
-            inside = fabsf(l[1]) <= P.he[1] && r2 <= mul(P.he[0], P.he[0]);
-        } else {
-            inside = fabsf(l[0]) <= P.he[0] && fabsf(l[1]) <= P.he[1] && fabsf(l[2]) <= P.he[2];
-        }
-        if (inside) {
-            const float vb[3] = {add(P.vl[0], sub(mul(P.w[1], r[2]), mul(P.w[2], r[1]))),
-                                 add(P.vl[1], sub(mul(P.w[2], r[0]), mul(P.w[0], r[2]))),
-                                 add(P.vl[2], sub(mul(P.w[0], r[1]), mul(P.w[1], r[0])))};
+        float r[3], vb[3];
+        if (m1_node_inside(P, dx, ox + li, oy + lj, oz + lk, r, vb)) {
             float4 nv = A.mv[id];
             float va[3];
             if (!(nv.w >= 1e-9f)) {  // inactive (mass 0) or mass < 1e-9: body claims the node

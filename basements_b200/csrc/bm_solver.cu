@@ -17,48 +17,15 @@
 #include <string>
 #include <vector>
 
-#include "bm_world.h"
+#include "bm_solver_impl.h"
 
 namespace bm {
 const char* last_error_text();
 }
 using namespace bm;
 
-struct bm_solver {
-    World w;
-    bool acc_valid = false;           // acc[cur] holds P2G of the current particle state
-    bool folded[2] = {false, false};  // acc[b].mv holds momentum + force * fold_dt[b]
-    float fold_dt[2] = {0.0f, 0.0f};
-    int view = 0;                     // buffer holding the grid a caller sees
-    int32_t sort_interval = 16;
-    int64_t steps_since_sort = 0;
-    bool sorted = false;
-    bool fast_math = false;
-    int variant = 1;  // 128 threads x 5 CTAs per SM: fastest on the 2M-particle wheel rut
-    // couplers
-    double* d_acc = nullptr;
-    bm_reaction_t* d_react = nullptr;
-    M1Params* d_params = nullptr;
-    int react_cap = 0;
-    std::vector<M1Params> h_params;
-
-    SceneHost& sc() { return w.scenes[0]; }
-};
-
-namespace {
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
+namespace bm {
+namespace sol {
 
 bm_status_t ensure_reactions(bm_solver* s, int n) {
     if (n <= s->react_cap) return BM_OK;
@@ -210,7 +177,10 @@ void invalidate_state(bm_solver* s) {
     s->sorted = false;
 }
 
-}  // namespace
+}  // namespace sol
+}  // namespace bm
+
+using namespace bm::sol;
 
 extern "C" {
 

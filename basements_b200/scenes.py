@@ -216,3 +216,110 @@ def serve_request_scene(seed: int) -> Scene:
     dom = ((-G // 2, -4, -G // 2), (2 * G, G + 8, 2 * G))
     return Scene(f"request_{seed}", dx, G, pos, np.full(len(pos), m, np.float32), E, nu, rho, dp_alpha(phi),
                  _stable_dt(E, nu, rho, dx), steps, bodies=bodies, domain=dom)
+
+
+def tine_pass(grid=64, bed_cells=(64, 16, 64), ppc=4, n_waypoints=16, steps=200, dt=1e-4,
+              tine_half=(0.01, 0.05, 0.025), depth=0.03, speed=1.0, jitter=2.5e-4, seed=0):
+    """Differentiable tine pass: a sand bed of bed_cells at `ppc` jittered
+    particles per cell (64 x 16 x 64 at 4 ppc = 262,144 particles on the
+    64^3 grid), the sand-column material at a 30 deg friction angle, and a
+    kinematic box tine (half extents 0.01 x 0.05 x 0.025 m, steel density)
+    dragged `depth` deep through the bed along +x at `speed` m/s; its path is
+    `n_waypoints` seeded control points (the straight drag plus N(0, jitter)
+    per coordinate), linearly interpolated over steps*dt. Returns
+    (scene, body template, waypoints (n_waypoints x 3, float32), target
+    heightfield (grid x grid, float64)); the target is the bed's initial
+    heightfield plus a seeded smooth bump pattern of +-2 mm."""
+    rng = np.random.default_rng(3000 + seed)
+    dx = 1.0 / grid
+    ci, cj, ck = bed_cells
+    ii, jj, kk = np.meshgrid(np.arange(ci), np.arange(cj), np.arange(ck), indexing="ij")
+    base = np.stack([ii, jj, kk], -1).reshape(-1, 3).astype(np.float32)
+    jit = rng.random((len(base), ppc, 3), dtype=np.float32)
+    pos = ((base[:, None, :] + jit) * np.float32(dx)).reshape(-1, 3)
+    rho, E, nu = 1600.0, 3.5e5, 0.3
+    m = np.float32(rho * dx ** 3 / ppc)
+    top = cj * dx
+    hx, hy, hz = tine_half
+    c0 = np.array([0.3, top - depth + hy, 0.5])
+    T = steps * float(np.float32(dt))
+    t = np.linspace(0.0, 1.0, n_waypoints)[:, None]
+    wp = c0[None, :] + t * np.array([speed * T, 0.0, 0.0])[None, :] + rng.normal(0.0, jitter, (n_waypoints, 3))
+    body = Body(center=tuple(map(float, wp[0])), half_extents=tuple(tine_half), orientation=(1.0, 0.0, 0.0, 0.0),
+                linear_velocity=(0.0, 0.0, 0.0), mass=float(7850.0 * 8 * hx * hy * hz), shape=0, kinematic=True)
+    h0 = heightfield(pos, grid)[0]
+    ph = rng.uniform(0, 2 * math.pi, 2)
+    u = (np.arange(grid) + 0.5) / grid
+    bump = 0.002 * np.sin(2 * math.pi * 3 * u[:, None] + ph[0]) * np.sin(2 * math.pi * 2 * u[None, :] + ph[1])
+    dom = ((-8, -4, -8), (grid + 16, int(0.6 * grid) + 8, grid + 16))
+    sc = Scene(f"tine_pass_{seed}", dx, grid, pos, np.full(len(pos), m, np.float32), E, nu, rho, dp_alpha(30.0),
+               float(np.float32(dt)), steps, bodies=[body], domain=dom)
+    return sc, body, wp.astype(np.float32), h0 + bump
+
+
+def body_on_path(body: Body, waypoints, n_steps: int, dt: float, n: int) -> Body:
+    """The body of step n on the piecewise-linear waypoint path spread over
+    n_steps*dt: centre on the path, linear velocity = the segment's slope
+    (double arithmetic, rounded to float32 at the end, as bm_tape_forward)."""
+    wp = np.asarray(waypoints, np.float32).astype(np.float64)
+    dt = float(np.float32(dt))
+    seg = (n_steps * dt) / (len(wp) - 1)
+    tn = n * dt
+    k = min(max(int(math.floor(tn / seg)), 0), len(wp) - 2)
+    v = [(wp[k + 1, a] - wp[k, a]) / seg for a in range(3)]
+    c = [wp[k, a] + (tn - k * seg) * v[a] for a in range(3)]
+    return Body(center=tuple(float(np.float32(x)) for x in c), half_extents=body.half_extents,
+                orientation=body.orientation, linear_velocity=tuple(float(np.float32(x)) for x in v),
+                angular_velocity=body.angular_velocity, friction=body.friction, mass=body.mass, shape=body.shape,
+                kinematic=body.kinematic)
+
+
+def heightfield(pos, nbins: int):
+    """Soft heightfield of particles over x, z in [0, 1): per bin b the
+    weighted mean height H_b = sum_p W_bp y_p / sum_p W_bp, W the bilinear
+    tent of one bin width around the bin centre (continuous in the
+    positions). Returns (H, S, parts) with S the weight sums; `parts` is kept
+    for heightfield_loss."""
+    p = np.asarray(pos, np.float64)
+    u = p[:, 0] * nbins - 0.5
+    w = p[:, 2] * nbins - 0.5
+    i0 = np.floor(u).astype(np.int64)
+    j0 = np.floor(w).astype(np.int64)
+    fu, fw = u - i0, w - j0
+    S = np.zeros(nbins * nbins)
+    Y = np.zeros(nbins * nbins)
+    parts = []
+    for di in (0, 1):
+        for dj in (0, 1):
+            bi, bj = i0 + di, j0 + dj
+            wu = fu if di else 1.0 - fu
+            wv = fw if dj else 1.0 - fw
+            ok = (bi >= 0) & (bi < nbins) & (bj >= 0) & (bj < nbins)
+            idx = np.where(ok, bi * nbins + bj, 0)
+            wt = np.where(ok, wu * wv, 0.0)
+            S += np.bincount(idx, wt, nbins * nbins)
+            Y += np.bincount(idx, wt * p[:, 1], nbins * nbins)
+            parts.append((idx, ok, wu, wv, 1.0 if di else -1.0, 1.0 if dj else -1.0))
+    H = np.where(S > 0, Y / np.where(S > 0, S, 1.0), 0.0)
+    return H.reshape(nbins, nbins), S.reshape(nbins, nbins), parts
+
+
+def heightfield_loss(pos, target):
+    """L = sum_b (H_b - target_b)^2 over the bins holding particles, and
+    dL/d position (n x 3, float64)."""
+    nbins = target.shape[0]
+    H, S, parts = heightfield(pos, nbins)
+    p = np.asarray(pos, np.float64)
+    live = S > 0
+    r = np.where(live, 2.0 * (H - target), 0.0).ravel()
+    Sf = np.where(live, S, 1.0).ravel()
+    Hf = H.ravel()
+    L = float(np.sum(np.where(live, (H - target) ** 2, 0.0)))
+    g = np.zeros_like(p)
+    for idx, ok, wu, wv, su, sv in parts:
+        rb = np.where(ok, r[idx] / Sf[idx], 0.0)
+        dy = p[:, 1] - Hf[idx]
+        g[:, 1] += rb * wu * wv
+        g[:, 0] += rb * dy * su * wv * nbins
+        g[:, 2] += rb * dy * wu * sv * nbins
+    return L, g

@@ -344,6 +344,41 @@ BM_API bm_status_t bm_server_stats(bm_server_t* s, bm_server_stats_t* out);
 /* Device bytes the admission policy charges for a scene. */
 BM_API bm_status_t bm_server_estimate_bytes(const bm_scene_desc_t* scene, double* bytes);
 
+/* ---- differentiable run --------------------------------------------------
+ * The reference declares AutodiffTape (mpm_autodiff_tape.h:37-92) and passes
+ * it to MPMSolver::step(dt, tape*) (mpm_solver.h:71-87), but the tape records
+ * nothing: there is no reference gradient. These calls give the split step
+ * (bm_solver_p2g, _grid_update, bm_coupler_m1_apply, _g2p) a reverse pass with
+ * hand-written adjoint kernels and checkpoints every K steps.
+ * Particle arrays are in add order, rows of 3 floats (9 for F and C). */
+typedef struct bm_tape bm_tape_t;
+/* A tape on solver s; checkpoint_every = K >= 1. The tape keeps
+ * ceil(n_steps/K)+1 checkpoints and K step states of 96 B per particle. */
+BM_API bm_status_t bm_tape_create(bm_solver_t* s, int32_t checkpoint_every, bm_tape_t** out);
+BM_API bm_status_t bm_tape_destroy(bm_tape_t* t);
+/* n_steps split steps from the solver's current particle state. With a
+ * body, its centre follows the piecewise-linear path through n_waypoints
+ * points (xyz each) spread evenly over n_steps*dt, its linear velocity is the
+ * slope of the current segment, everything else stays as in *body; body NULL:
+ * no coupler. The solver ends in the final state. */
+BM_API bm_status_t bm_tape_forward(bm_tape_t* t, float dt, int32_t n_steps, const bm_collider_t* body,
+                                   int32_t n_waypoints, const float* waypoints);
+/* Reverse pass of the last bm_tape_forward. dL_dx (required) and dL_dv (or
+ * NULL) are the loss gradient at the final state; outputs, each may be NULL:
+ * dL_dwaypoints (n_waypoints x 3), dL_dx0 and dL_dv0 (gradient at the initial
+ * state). The solver is left in the final state. */
+BM_API bm_status_t bm_adjoint_backward(bm_tape_t* t, const float* dL_dx, const float* dL_dv,
+                                       float* dL_dwaypoints, float* dL_dx0, float* dL_dv0);
+/* The same reverse pass for the whole particle state: dL_dfinal holds the
+ * loss gradient at the final state (position/velocity n x 3, F/C n x 9; NULL
+ * fields are zero, mass/volume ignored); dL_dinitial (or NULL) receives the
+ * gradient at the initial state in the fields it points to. */
+BM_API bm_status_t bm_adjoint_backward_state(bm_tape_t* t, const bm_particles_view_t* dL_dfinal,
+                                             float* dL_dwaypoints, const bm_particles_view_t* dL_dinitial);
+/* dL/d(body linear velocity) and dL/d(body angular velocity) of every step
+ * of the last backward pass: n_steps x 6 doubles. */
+BM_API bm_status_t bm_tape_body_grad(bm_tape_t* t, int32_t n_steps, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,6 +83,7 @@ def load(kind: str):
         "num_particles": fn("num_particles", C.c_int64, C.c_void_p),
         "set_particle_state": fn("set_particle_state", None, C.c_void_p, C.c_int64, C.c_int64, _f, _f, _f, _f),
         "get_particles": fn("get_particles", None, C.c_void_p, _f, _f, _f, _f, _f, _f),
+        "get_state_f64": fn("get_state_f64", None, C.c_void_p, *([C.POINTER(C.c_double)] * 4)),
         "step": fn("step", None, C.c_void_p, C.c_float, C.c_int),
         "p2g": fn("p2g", None, C.c_void_p, C.c_float),
         "grid_update": fn("grid_update", None, C.c_void_p, C.c_float),
@@ -178,6 +179,19 @@ class CpuSolver:
         }
         self.api["get_particles"](self.h, *[_p(out[k]) for k in ("position", "velocity", "F", "C", "mass", "volume")])
         return out
+
+    def state_f64(self):
+        """x, v (n x 3) and F, C (n x 3 x 3) in the solver's own precision, as double."""
+        n = self.num_particles()
+        out = {"position": np.empty((n, 3)), "velocity": np.empty((n, 3)), "F": np.empty((n, 3, 3)),
+               "C": np.empty((n, 3, 3))}
+        dp = C.POINTER(C.c_double)
+        self.api["get_state_f64"](self.h, *[out[k].ctypes.data_as(dp) for k in ("position", "velocity", "F", "C")])
+        return out
+
+    def positions_f64(self):
+        """Positions in the solver's own precision, as double."""
+        return self.state_f64()["position"]
 
     def step(self, dt, n_steps=1):
         self.api["step"](self.h, dt, int(n_steps))

@@ -88,6 +88,23 @@ ORC_EXPORT void orc_get_particles(void* h, float* pos, float* vel, float* F, flo
     }
 }
 
+ORC_EXPORT void orc_get_state_f64(void* h, double* pos, double* vel, double* F, double* C) {
+    int64_t q = 0;
+    for (const auto& p : sv(h)->particles) {
+        const double x[3] = {(double)p.x.x, (double)p.x.y, (double)p.x.z};
+        const double v[3] = {(double)p.v.x, (double)p.v.y, (double)p.v.z};
+        for (int a = 0; a < 3; ++a) {
+            if (pos) pos[3 * q + a] = x[a];
+            if (vel) vel[3 * q + a] = v[a];
+        }
+        for (int a = 0; a < 9; ++a) {
+            if (F) F[9 * q + a] = (double)p.F.m[a / 3][a % 3];
+            if (C) C[9 * q + a] = (double)p.C.m[a / 3][a % 3];
+        }
+        ++q;
+    }
+}
+
 ORC_EXPORT void orc_step(void* h, float dt, int n_steps) {
     for (int i = 0; i < n_steps; ++i) sv(h)->step(dt);
 }

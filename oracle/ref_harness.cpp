@@ -83,6 +83,23 @@ ORC_EXPORT void ref_set_particle_state(void* h, int64_t first, int64_t n, const 
     }
 }
 
+ORC_EXPORT void ref_get_state_f64(void* h, double* pos, double* vel, double* F, double* C) {
+    int64_t q = 0;
+    for (const auto& p : sv(h)->get_particles()) {
+        const float x[3] = {p.position.x, p.position.y, p.position.z};
+        const float v[3] = {p.velocity.x, p.velocity.y, p.velocity.z};
+        for (int a = 0; a < 3; ++a) {
+            if (pos) pos[3 * q + a] = x[a];
+            if (vel) vel[3 * q + a] = v[a];
+        }
+        for (int a = 0; a < 9; ++a) {
+            if (F) F[9 * q + a] = p.F.m[a / 3][a % 3];
+            if (C) C[9 * q + a] = p.C.m[a / 3][a % 3];
+        }
+        ++q;
+    }
+}
+
 ORC_EXPORT void ref_get_particles(void* h, float* pos, float* vel, float* F, float* C, float* mass, float* vol) {
     int64_t q = 0;
     for (const auto& p : sv(h)->get_particles()) {
