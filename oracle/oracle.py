@@ -84,6 +84,8 @@ def load(kind: str):
         "set_particle_state": fn("set_particle_state", None, C.c_void_p, C.c_int64, C.c_int64, _f, _f, _f, _f),
         "get_particles": fn("get_particles", None, C.c_void_p, _f, _f, _f, _f, _f, _f),
         "get_state_f64": fn("get_state_f64", None, C.c_void_p, *([C.POINTER(C.c_double)] * 4)),
+        "set_state_f64": fn("set_state_f64", None, C.c_void_p, C.c_int64, C.c_int64,
+                            *([C.POINTER(C.c_double)] * 4)),
         "step": fn("step", None, C.c_void_p, C.c_float, C.c_int),
         "p2g": fn("p2g", None, C.c_void_p, C.c_float),
         "grid_update": fn("grid_update", None, C.c_void_p, C.c_float),
@@ -188,6 +190,14 @@ class CpuSolver:
         dp = C.POINTER(C.c_double)
         self.api["get_state_f64"](self.h, *[out[k].ctypes.data_as(dp) for k in ("position", "velocity", "F", "C")])
         return out
+
+    def set_state_f64(self, pos=None, vel=None, F=None, C_=None):
+        """Overwrite x, v, F, C of all particles from double arrays (the f64
+        solver keeps them in double; the float ones round)."""
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (pos, vel, F, C_)]
+        dp = C.POINTER(C.c_double)
+        self.api["set_state_f64"](self.h, 0, self.num_particles(),
+                                  *[None if a is None else a.ctypes.data_as(dp) for a in arrs])
 
     def positions_f64(self):
         """Positions in the solver's own precision, as double."""

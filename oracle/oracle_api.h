@@ -50,6 +50,9 @@ ORC_EXPORT void ORC(get_particles)(void* h, float* pos, float* vel, float* F, fl
 /* x, v (n x 3), F, C (n x 9, row-major) in the solver's own precision,
  * widened to double; NULL skips a field */
 ORC_EXPORT void ORC(get_state_f64)(void* h, double* pos, double* vel, double* F, double* C);
+/* set_particle_state from double arrays (rounded to the solver's precision) */
+ORC_EXPORT void ORC(set_state_f64)(void* h, int64_t first, int64_t n, const double* pos, const double* vel,
+                                   const double* F, const double* C);
 ORC_EXPORT void ORC(step)(void* h, float dt, int n_steps);
 ORC_EXPORT void ORC(p2g)(void* h, float dt);
 ORC_EXPORT void ORC(grid_update)(void* h, float dt);

@@ -72,6 +72,20 @@ ORC_EXPORT void orc_set_particle_state(void* h, int64_t first, int64_t n, const 
     }
 }
 
+ORC_EXPORT void orc_set_state_f64(void* h, int64_t first, int64_t n, const double* pos, const double* vel,
+                                  const double* F, const double* C) {
+    S* s = sv(h);
+    for (int64_t q = 0; q < n; ++q) {
+        Particle<R>& p = s->particles[first + q];
+        if (pos) p.x = V3<R>((R)pos[3 * q], (R)pos[3 * q + 1], (R)pos[3 * q + 2]);
+        if (vel) p.v = V3<R>((R)vel[3 * q], (R)vel[3 * q + 1], (R)vel[3 * q + 2]);
+        for (int a = 0; a < 9; ++a) {
+            if (F) p.F.m[a / 3][a % 3] = (R)F[9 * q + a];
+            if (C) p.C.m[a / 3][a % 3] = (R)C[9 * q + a];
+        }
+    }
+}
+
 ORC_EXPORT void orc_get_particles(void* h, float* pos, float* vel, float* F, float* C, float* mass, float* vol) {
     S* s = sv(h);
     int64_t q = 0;

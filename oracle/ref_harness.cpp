@@ -83,6 +83,20 @@ ORC_EXPORT void ref_set_particle_state(void* h, int64_t first, int64_t n, const 
     }
 }
 
+ORC_EXPORT void ref_set_state_f64(void* h, int64_t first, int64_t n, const double* pos, const double* vel,
+                                  const double* F, const double* C) {
+    auto& ps = sv(h)->get_particles_mutable();
+    for (int64_t q = 0; q < n; ++q) {
+        mpm::Particle& p = ps[first + q];
+        if (pos) p.position = Vec3((float)pos[3 * q], (float)pos[3 * q + 1], (float)pos[3 * q + 2]);
+        if (vel) p.velocity = Vec3((float)vel[3 * q], (float)vel[3 * q + 1], (float)vel[3 * q + 2]);
+        for (int a = 0; a < 9; ++a) {
+            if (F) p.F.m[a / 3][a % 3] = (float)F[9 * q + a];
+            if (C) p.C.m[a / 3][a % 3] = (float)C[9 * q + a];
+        }
+    }
+}
+
 ORC_EXPORT void ref_get_state_f64(void* h, double* pos, double* vel, double* F, double* C) {
     int64_t q = 0;
     for (const auto& p : sv(h)->get_particles()) {
