@@ -29,7 +29,8 @@ struct bm_batch {
     double* d_acc = nullptr;
     bm_reaction_t* d_react = nullptr;
     int n_bodies = 0;
-    int64_t max_cand = 0;
+    std::vector<int64_t> h_cand_prefix{0};  // body b owns M1 CTAs [prefix[b], prefix[b+1])
+    int64_t* d_cand_prefix = nullptr;
     int64_t steps_done = 0;
     bool started = false;  // P2G of the first step done
     int32_t sort_interval = 16;
@@ -78,7 +79,8 @@ bm_status_t eager_step(bm_batch* b) {
         BM_CHECK_CUDA(cudaMemsetAsync(b->d_acc, 0, sizeof(double) * 7 * b->n_bodies, w.stream));
         w.timed("m1_coupler", [&] {
             launch_body_prepare(w.table(), b->d_bodies, b->n_bodies, b->d_params, w.stream);
-            launch_m1(w.table(), b->d_params, b->n_bodies, b->max_cand, w.cur, b->d_acc, w.stream);
+            launch_m1_flat(w.table(), b->d_params, b->n_bodies, b->d_cand_prefix, b->h_cand_prefix.back(), w.cur,
+                           b->d_acc, w.stream);
             launch_body_integrate(b->d_bodies, b->n_bodies, b->d_acc, w.stream);
             launch_reaction_finalize(b->d_acc, b->n_bodies, b->d_react, w.stream);
         });
@@ -316,7 +318,7 @@ BM_API bm_status_t bm_batch_create(int32_t n_scenes, const bm_scene_desc_t* scen
             B.scene = i;
             body = (int)b->h_bodies.size();
             b->h_bodies.push_back(B);
-            b->max_cand = std::max(b->max_cand, m1_max_candidates(h.dev.g, d.body.half_extents));
+            b->h_cand_prefix.push_back(b->h_cand_prefix.back() + m1_max_candidates(h.dev.g, d.body.half_extents));
         }
         b->body_of_scene.push_back(body);
     }
@@ -326,7 +328,8 @@ BM_API bm_status_t bm_batch_create(int32_t n_scenes, const bm_scene_desc_t* scen
         if (cudaMalloc((void**)&b->d_bodies, sizeof(BodyDev) * nb) != cudaSuccess ||
             cudaMalloc((void**)&b->d_params, sizeof(M1Params) * nb) != cudaSuccess ||
             cudaMalloc((void**)&b->d_acc, sizeof(double) * 7 * nb) != cudaSuccess ||
-            cudaMalloc((void**)&b->d_react, sizeof(bm_reaction_t) * nb) != cudaSuccess) {
+            cudaMalloc((void**)&b->d_react, sizeof(bm_reaction_t) * nb) != cudaSuccess ||
+            cudaMalloc((void**)&b->d_cand_prefix, sizeof(int64_t) * (nb + 1)) != cudaSuccess) {
             set_last_error("batch body buffers");
             st = BM_ERR_OUT_OF_MEMORY;
         }
@@ -336,6 +339,9 @@ BM_API bm_status_t bm_batch_create(int32_t n_scenes, const bm_scene_desc_t* scen
             cudaSuccess)
             st = BM_ERR_CUDA;
         cudaMemset(b->d_react, 0, sizeof(bm_reaction_t) * b->n_bodies);
+        if (cudaMemcpy(b->d_cand_prefix, b->h_cand_prefix.data(), sizeof(int64_t) * b->h_cand_prefix.size(),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            st = BM_ERR_CUDA;
     }
     if (st == BM_OK) st = w.sync_table();
     if (st == BM_OK && cudaStreamSynchronize(w.stream) != cudaSuccess) st = BM_ERR_CUDA;
@@ -356,6 +362,7 @@ BM_API bm_status_t bm_batch_destroy(bm_batch_t* b) {
     cudaFree(b->d_params);
     cudaFree(b->d_acc);
     cudaFree(b->d_react);
+    cudaFree(b->d_cand_prefix);
     delete b;
     return BM_OK;
 }

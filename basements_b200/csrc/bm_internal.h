@@ -225,6 +225,10 @@ void launch_gather_rows(const ParticleSoA& ps, int plane0, int width, float* out
 void launch_scatter_rows(const ParticleSoA& ps, int plane0, int width, const float* in_rows, int64_t first,
                          int64_t n, const int32_t* inv, cudaStream_t st);
 void launch_inverse_pid(const ParticleSoA& ps, int32_t* inv, cudaStream_t st);
+// Particles [n0, n0 + n) of a store from device rows (pos n x 3, vel n x 3 or
+// NULL, mass n or NULL): F = I, C = 0, V0 = m / density, pid = slot.
+void launch_fill_particles(const ParticleSoA& s, int64_t n0, int64_t n, const float* pos, const float* vel,
+                           const float* mass, float density, cudaStream_t st);
 
 // ---- coupler and bodies (bm_m1.cu) ------------------------------------------------
 // M1 parameters of one body for one step, computed on the host
@@ -253,6 +257,10 @@ int64_t m1_max_candidates(const GridDesc& g, const float half_extents[3]);
 // One CTA of 64 threads per candidate block: grid (max_candidates, n_bodies).
 void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int64_t max_candidates, int cur,
                double* d_acc, cudaStream_t st);
+// Flat grid: body b owns CTAs [d_cand_prefix[b], d_cand_prefix[b+1]) (each an
+// upper bound of its candidate blocks, e.g. m1_max_candidates), total CTAs.
+void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies, const int64_t* d_cand_prefix,
+                    int64_t total_candidates, int cur, double* d_acc, cudaStream_t st);
 void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st);
 
 // Rigid bodies stepped on the device (batched and served forms), with the

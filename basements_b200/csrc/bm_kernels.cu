@@ -41,8 +41,14 @@ constexpr int kGridThreads = 256;
 constexpr int kScanThreads = 1024;
 constexpr int kScanTile = kScanThreads * 8;
 
+// 16-byte vector reduction into global memory, no value returned. Written as
+// PTX with the global state space: a pointer the compiler cannot prove
+// global (one read from a scene table) otherwise becomes a generic atomic
+// that returns its old value, which doubled the crossbar traffic and kept
+// L1 busy checking the shared window.
 __device__ __forceinline__ void red_v4(float4* a, float x, float y, float z, float w) {
-    atomicAdd(a, make_float4(x, y, z, w));
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(a), "f"(x), "f"(y), "f"(z), "f"(w)
+                 : "memory");
 }
 
 // a[i] for a runtime i in {0,1,2} without indexing (keeps `a` in registers).
@@ -503,21 +509,34 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
 }
 
 // Many scenes: the view of each 128-thread unit's scene comes from the CTA
-// prefix table.
+// prefix table. Every unit belongs to one scene; its first thread copies the
+// view into shared memory, so the scene's fields are read from there (a view
+// read through a global pointer stays live in registers and made this kernel
+// spill four to six times more than the single-scene one).
 template <bool Fast, int Threads, int MinBlocks>
 __global__ void __launch_bounds__(Threads, MinBlocks)
     k_g2p2g(const FusedScene* __restrict__ views, const int64_t* __restrict__ prefix, int n_scenes) {
+    constexpr int kUnitThreads = Threads < kParticleCTA ? Threads : kParticleCTA;
+    constexpr int kUnits = Threads / kUnitThreads;
+    __shared__ FusedScene sview[kUnits];
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t unit = gtid / kParticleCTA;
-    if (unit >= prefix[n_scenes]) return;
-    int lo = 0, hi = n_scenes - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= unit) lo = mid;
-        else hi = mid - 1;
+    const int u = (int)threadIdx.x / kUnitThreads;
+    const bool live = unit < prefix[n_scenes];
+    int lo = 0;
+    if (live) {
+        int hi = n_scenes - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= unit) lo = mid;
+            else hi = mid - 1;
+        }
+        if (threadIdx.x % kUnitThreads == 0) sview[u] = views[lo];
     }
+    __syncthreads();
+    if (!live) return;
     const int64_t p = (unit - prefix[lo]) * kParticleCTA + (gtid % kParticleCTA);
-    const FusedScene& S = views[lo];
+    const FusedScene& S = sview[u];
     if (p >= S.n) return;
     g2p2g_particle<Fast>(S, p);
 }
@@ -688,6 +707,30 @@ __global__ void k_inverse_pid(ParticleSoA ps, int32_t* inv) {
     inv[ps.pid[p]] = (int32_t)p;
 }
 
+// New particles [n0, n0 + n) of a store from the caller's rows: F = I,
+// C = 0, V0 = m / rho (mpm_solver.h:23-34, the reference's add_particle).
+// vel / mass NULL: zero velocity / mass 1.
+__global__ void k_fill_particles(ParticleSoA s, int64_t n0, int64_t n, const float* __restrict__ pos,
+                                 const float* __restrict__ vel, const float* __restrict__ mass, float density) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int64_t p = n0 + q;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        s.plane(P_X + a)[p] = pos[3 * q + a];
+        s.plane(P_V + a)[p] = vel ? vel[3 * q + a] : 0.0f;
+    }
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+        s.plane(P_F + a)[p] = (a % 4 == 0) ? 1.0f : 0.0f;
+        s.plane(P_C + a)[p] = 0.0f;
+    }
+    const float m = mass ? mass[q] : 1.0f;
+    s.plane(P_M)[p] = m;
+    s.plane(P_V0)[p] = (density > 1e-12f) ? (m / density) : 1.0f;
+    s.pid[p] = (int32_t)p;
+}
+
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // Compiled launch shapes of the fused kernel: threads per CTA and the
@@ -786,6 +829,12 @@ void launch_scatter_rows(const ParticleSoA& ps, int plane0, int width, const flo
                          const int32_t* inv, cudaStream_t st) {
     if (n == 0) return;
     k_scatter_rows<<<nblk(n, 256), 256, 0, st>>>(ps, plane0, width, in, first, n, inv);
+}
+
+void launch_fill_particles(const ParticleSoA& s, int64_t n0, int64_t n, const float* pos, const float* vel,
+                           const float* mass, float density, cudaStream_t st) {
+    if (n <= 0) return;
+    k_fill_particles<<<nblk(n, 256), 256, 0, st>>>(s, n0, n, pos, vel, mass, density);
 }
 
 void launch_inverse_pid(const ParticleSoA& ps, int32_t* inv, cudaStream_t st) {

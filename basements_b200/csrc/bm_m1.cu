@@ -62,8 +62,9 @@ __host__ __device__ bool m1_params(const GridDesc& g, const bm_collider_t& b, fl
     int b0[3], n[3];
     for (int a = 0; a < 3; ++a) {
         if (!(P->lo[a] > -1e30f && P->hi[a] < 1e30f)) return false;
-        const double lo_node = floor((double)P->lo[a] / dx - 0.5) - 4;
-        const double hi_node = ceil((double)P->hi[a] / dx - 0.5) + 4;
+        // one node of slack on each side for the float/double rounding
+        const double lo_node = floor((double)P->lo[a] / dx - 0.5) - 1;
+        const double hi_node = ceil((double)P->hi[a] / dx - 0.5) + 1;
         double lo_b = floor((lo_node - org[a]) / 4.0);
         double hi_b = floor((hi_node - org[a]) / 4.0);
         lo_b = lo_b < 0.0 ? 0.0 : lo_b;
@@ -78,16 +79,31 @@ __host__ __device__ bool m1_params(const GridDesc& g, const bm_collider_t& b, fl
     return true;
 }
 
-__global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params, int cur, double* acc_all) {
-    const M1Params& P = params[blockIdx.y];
+// cand_prefix NULL: grid (max candidates, bodies), body = blockIdx.y.
+// Otherwise a flat grid over the bodies' candidate bounds: body b owns CTAs
+// [cand_prefix[b], cand_prefix[b+1]).
+__global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params, int cur, double* acc_all,
+                                           const int64_t* __restrict__ cand_prefix, int n_bodies) {
+    int body = blockIdx.y;
+    int64_t cb = blockIdx.x;
+    if (cand_prefix) {
+        int lo = 0, hi = n_bodies - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cand_prefix[mid] <= (int64_t)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        body = lo;
+        cb = (int64_t)blockIdx.x - cand_prefix[lo];
+    }
+    const M1Params& P = params[body];
     if (!P.active) return;
     const int64_t ncand = (int64_t)P.nbi * P.nbj * P.nbk;
-    const int64_t cb = blockIdx.x;
     if (cb >= ncand) return;
     const SceneDev& S = t.scenes[P.scene];
     const GridDesc g = S.g;
     const GridAcc A = S.acc[cur];
-    double* acc = acc_all + 7 * blockIdx.y;
+    double* acc = acc_all + 7 * body;
     const int bk = P.bk0 + (int)(cb % P.nbk);
     const int bj = P.bj0 + (int)((cb / P.nbk) % P.nbj);
     const int bi = P.bi0 + (int)(cb / ((int64_t)P.nbk * P.nbj));
@@ -259,9 +275,11 @@ bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, int scene, 
 }
 
 int64_t m1_max_candidates(const GridDesc& g, const float he[3]) {
-    // each AABB half side is at most hx + hy + hz (|R_ij| <= 1)
-    const double h = (double)std::fabs(he[0]) + std::fabs(he[1]) + std::fabs(he[2]);
-    const double nodes = 2.0 * h / g.dx + 12.0;
+    // each AABB half side is sum_j |R_aj| h_j <= |h| (a row of R has unit
+    // length); the candidate nodes span at most 2 |h| / dx + 4 (rounding and
+    // one node of slack each side), i.e. span / 4 + 2 blocks per axis
+    const double h = std::sqrt((double)he[0] * he[0] + (double)he[1] * he[1] + (double)he[2] * he[2]) * (1.0 + 1e-6);
+    const double nodes = 2.0 * h / g.dx + 4.0;
     const int64_t per = (int64_t)std::ceil(nodes / 4.0) + 2;
     const int64_t a = std::min<int64_t>(per, g.nbx), b = std::min<int64_t>(per, g.nby), c = std::min<int64_t>(per, g.nbz);
     return std::max<int64_t>(1, a * b * c);
@@ -270,7 +288,14 @@ int64_t m1_max_candidates(const GridDesc& g, const float he[3]) {
 void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int64_t max_candidates, int cur,
                double* d_acc, cudaStream_t st) {
     if (n_bodies <= 0 || max_candidates <= 0) return;
-    k_m1<<<dim3((unsigned)max_candidates, (unsigned)n_bodies), 64, 0, st>>>(t, d_params, cur, d_acc);
+    k_m1<<<dim3((unsigned)max_candidates, (unsigned)n_bodies), 64, 0, st>>>(t, d_params, cur, d_acc, nullptr,
+                                                                             n_bodies);
+}
+
+void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies, const int64_t* d_cand_prefix,
+                    int64_t total_candidates, int cur, double* d_acc, cudaStream_t st) {
+    if (n_bodies <= 0 || total_candidates <= 0) return;
+    k_m1<<<(unsigned)total_candidates, 64, 0, st>>>(t, d_params, cur, d_acc, d_cand_prefix, n_bodies);
 }
 
 void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st) {

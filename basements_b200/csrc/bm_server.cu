@@ -94,7 +94,10 @@ struct bm_server {
     double* d_acc = nullptr;
     bm_reaction_t* d_react = nullptr;
     int body_cap = 0;
-    int64_t max_cand = 0;
+    int64_t* d_cand_prefix = nullptr;  // body b owns M1 CTAs [prefix[b], prefix[b+1])
+    int64_t total_cand = 0;
+    float* h_stage = nullptr;  // pinned read-back staging of finished scenes
+    size_t stage_cap = 0;      // floats
     double used_bytes = 0;
     // shared state
     std::mutex mu;
@@ -118,7 +121,7 @@ namespace {
 bm_status_t rebuild_bodies(bm_server* s) {
     World& w = s->w;
     std::vector<BodyDev> next;
-    s->max_cand = 0;
+    std::vector<int64_t> prefix(1, 0);
     for (size_t i = 0; i < s->active.size(); ++i) {
         const Request& r = *s->active[i].req;
         if (!r.desc.has_body) continue;
@@ -134,7 +137,7 @@ bm_status_t rebuild_bodies(bm_server* s) {
         B.dynamic = r.desc.body_dynamic;
         B.scene = (int32_t)i;
         next.push_back(B);
-        s->max_cand = std::max(s->max_cand, m1_max_candidates(w.scenes[i].dev.g, r.desc.body.half_extents));
+        prefix.push_back(prefix.back() + m1_max_candidates(w.scenes[i].dev.g, r.desc.body.half_extents));
     }
     s->h_bodies = next;
     if ((int)next.size() > s->body_cap) {
@@ -142,16 +145,27 @@ bm_status_t rebuild_bodies(bm_server* s) {
         cudaFree(s->d_params);
         cudaFree(s->d_acc);
         cudaFree(s->d_react);
+        cudaFree(s->d_cand_prefix);
+        s->d_bodies = nullptr;
+        s->d_params = nullptr;
+        s->d_acc = nullptr;
+        s->d_react = nullptr;
+        s->d_cand_prefix = nullptr;
         const int cap = std::max<int>((int)next.size(), s->body_cap * 2);
         BM_CHECK_CUDA(cudaMalloc((void**)&s->d_bodies, sizeof(BodyDev) * cap));
         BM_CHECK_CUDA(cudaMalloc((void**)&s->d_params, sizeof(M1Params) * cap));
         BM_CHECK_CUDA(cudaMalloc((void**)&s->d_acc, sizeof(double) * 7 * cap));
         BM_CHECK_CUDA(cudaMalloc((void**)&s->d_react, sizeof(bm_reaction_t) * cap));
+        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_cand_prefix, sizeof(int64_t) * (cap + 1)));
         s->body_cap = cap;
     }
-    if (!next.empty())
+    s->total_cand = prefix.back();
+    if (!next.empty()) {
         BM_CHECK_CUDA(cudaMemcpyAsync(s->d_bodies, next.data(), sizeof(BodyDev) * next.size(), cudaMemcpyHostToDevice,
                                       w.stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_cand_prefix, prefix.data(), sizeof(int64_t) * prefix.size(),
+                                      cudaMemcpyHostToDevice, w.stream));
+    }
     BM_CHECK_CUDA(cudaStreamSynchronize(w.stream));
     return BM_OK;
 }
@@ -215,22 +229,33 @@ bm_status_t collect(bm_server* s, int i) {
     r.out_vel.resize(3 * n);
     r.out_F.resize(9 * n);
     r.out_C.resize(9 * n);
+    // x, v, F, C rows land in pinned memory (a pageable read-back is several
+    // times slower and holds the worker while other scenes wait)
+    const size_t need = (size_t)24 * std::max<int64_t>(n, 1);
+    if (need > s->stage_cap) {
+        cudaFreeHost(s->h_stage);
+        s->h_stage = nullptr;
+        s->stage_cap = 0;
+        BM_CHECK_CUDA(cudaMallocHost((void**)&s->h_stage, sizeof(float) * need));
+        s->stage_cap = need;
+    }
+    struct Fld { std::vector<float>* dst; int plane; int width; size_t off; };
+    const Fld fs[] = {{&r.out_pos, P_X, 3, 0}, {&r.out_vel, P_V, 3, 3 * (size_t)n}, {&r.out_F, P_F, 9, 6 * (size_t)n},
+                      {&r.out_C, P_C, 9, 15 * (size_t)n}};
     if (n > 0) {
         float* tmp = nullptr;
-        BM_CHECK_CUDA(cudaMallocAsync((void**)&tmp, sizeof(float) * 9 * n, w.stream));
+        BM_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&tmp, sizeof(float) * 24 * n, w.pool, w.stream));
         const ParticleSoA& ps = h.dev.store[w.sel];
-        struct F { float* dst; int plane; int width; };
-        const F fs[] = {{r.out_pos.data(), P_X, 3}, {r.out_vel.data(), P_V, 3}, {r.out_F.data(), P_F, 9},
-                        {r.out_C.data(), P_C, 9}};
-        for (const F& f : fs) {
-            launch_gather_rows(ps, f.plane, f.width, tmp, w.stream);
-            BM_CHECK_CUDA(cudaMemcpyAsync(f.dst, tmp, sizeof(float) * f.width * n, cudaMemcpyDeviceToHost, w.stream));
-        }
+        for (const Fld& f : fs) launch_gather_rows(ps, f.plane, f.width, tmp + f.off, w.stream);
+        BM_CHECK_CUDA(cudaMemcpyAsync(s->h_stage, tmp, sizeof(float) * 24 * n, cudaMemcpyDeviceToHost, w.stream));
         cudaFreeAsync(tmp, w.stream);
     }
     uint32_t status = 0;
     BM_CHECK_CUDA(cudaMemcpyAsync(&status, h.dev.status, sizeof(status), cudaMemcpyDeviceToHost, w.stream));
     BM_CHECK_CUDA(cudaStreamSynchronize(w.stream));
+    if (n > 0)
+        for (const Fld& f : fs)
+            std::memcpy(f.dst->data(), s->h_stage + f.off, sizeof(float) * f.width * n);
     r.error = (status & ERR_NONFINITE) ? BM_ERR_NON_FINITE : (status & ERR_ESCAPE) ? BM_ERR_DOMAIN_ESCAPE : BM_OK;
     return BM_OK;
 }
@@ -247,7 +272,7 @@ bm_status_t step_all(bm_server* s, bool admitted) {
         const int nb = (int)s->h_bodies.size();
         BM_CHECK_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(double) * 7 * nb, w.stream));
         launch_body_prepare(w.table(), s->d_bodies, nb, s->d_params, w.stream);
-        launch_m1(w.table(), s->d_params, nb, s->max_cand, w.cur, s->d_acc, w.stream);
+        launch_m1_flat(w.table(), s->d_params, nb, s->d_cand_prefix, s->total_cand, w.cur, s->d_acc, w.stream);
         launch_body_integrate(s->d_bodies, nb, s->d_acc, w.stream);
         st = launch_status("server coupler");
     }
@@ -420,6 +445,8 @@ BM_API bm_status_t bm_server_destroy(bm_server_t* s) {
     cudaFree(s->d_params);
     cudaFree(s->d_acc);
     cudaFree(s->d_react);
+    cudaFree(s->d_cand_prefix);
+    cudaFreeHost(s->h_stage);
     delete s;
     return BM_OK;
 }

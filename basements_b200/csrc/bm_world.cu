@@ -42,11 +42,12 @@ GridDesc desc_from_domain(const bm_domain_t& d, float dx) {
     return g;
 }
 
+// Stream-ordered allocation from the World's pool (freed with cudaFreeAsync).
 template <class T>
-bm_status_t dmalloc(T** p, size_t n, cudaStream_t st) {
+bm_status_t dmalloc(T** p, size_t n, cudaStream_t st, cudaMemPool_t pool) {
     *p = nullptr;
     if (n == 0) n = 1;
-    BM_CHECK_CUDA(cudaMallocAsync((void**)p, sizeof(T) * n, st));
+    BM_CHECK_CUDA(cudaMallocFromPoolAsync((void**)p, sizeof(T) * n, pool, st));
     return BM_OK;
 }
 
@@ -62,30 +63,45 @@ bm_status_t World::init() {
     BM_CHECK_CUDA(cudaGetDevice(&device));
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
     BM_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    // Scene buffers come from a pool of this World that keeps freed memory
+    // for the next scene: the served form admits and retires scenes all the
+    // time, and returning the memory to the driver at every synchronisation
+    // (the default pool's behaviour) made each admission map hundreds of MB
+    // afresh.
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    BM_CHECK_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = UINT64_MAX;
+    BM_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     return BM_OK;
 }
 
 void World::free_scene(SceneHost& h) {
     SceneDev& d = h.dev;
+    auto drop = [&](void* p) {
+        if (p) cudaFreeAsync(p, stream);
+    };
     for (auto& s : d.store) {
-        cudaFree(s.base);
-        cudaFree(s.pid);
+        drop(s.base);
+        drop(s.pid);
         s = ParticleSoA{nullptr, nullptr, 0, 0};
     }
     for (auto& a : d.acc) {
-        cudaFree(a.mv);
-        cudaFree(a.f);
-        cudaFree(a.touched);
-        cudaFree(a.list);
-        cudaFree(a.count);
+        drop(a.mv);
+        drop(a.f);
+        drop(a.touched);
+        drop(a.list);
+        drop(a.count);
         a = GridAcc{};
     }
-    cudaFree(d.alloc);
-    cudaFree(d.key);
-    cudaFree(d.rank);
-    cudaFree(d.status);
-    cudaFree(d.escaped);
-    cudaFree(h.d_inv);
+    drop(d.alloc);
+    drop(d.key);
+    drop(d.rank);
+    drop(d.status);
+    drop(d.escaped);
+    drop(h.d_inv);
     d.alloc = nullptr;
     d.key = d.rank = nullptr;
     d.status = nullptr;
@@ -120,14 +136,16 @@ void World::release() {
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
     t0 = t1 = nullptr;
+    if (stream) cudaStreamSynchronize(stream);
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
+    if (pool) cudaMemPoolDestroy(pool);
+    pool = nullptr;
 }
 
 void World::remove_scene(int index) {
     if (index < 0 || index >= (int)scenes.size()) return;
-    cudaStreamSynchronize(stream);
-    free_scene(scenes[index]);
+    free_scene(scenes[index]);  // stream-ordered: after the work already queued
     scenes.erase(scenes.begin() + index);
     dirty = true;
 }
@@ -140,8 +158,7 @@ bm_status_t World::p2g_fresh() {
 int World::add_scene() {
     scenes.emplace_back();
     SceneHost& h = scenes.back();
-    if (cudaMalloc((void**)&h.dev.status, sizeof(uint32_t)) == cudaSuccess &&
-        cudaMalloc((void**)&h.dev.escaped, sizeof(unsigned long long)) == cudaSuccess) {
+    if (dmalloc(&h.dev.status, 1, stream, pool) == BM_OK && dmalloc(&h.dev.escaped, 1, stream, pool) == BM_OK) {
         cudaMemsetAsync(h.dev.status, 0, sizeof(uint32_t), stream);
         cudaMemsetAsync(h.dev.escaped, 0, sizeof(unsigned long long), stream);
     }
@@ -171,8 +188,8 @@ bm_status_t World::ensure_particle_capacity(SceneHost& h, int64_t need) {
     ParticleSoA fresh[2];
     for (int s = 0; s < 2; ++s) {
         fresh[s] = ParticleSoA{nullptr, nullptr, cap, n};
-        bm_status_t st = dmalloc(&fresh[s].base, (size_t)N_PLANES * cap, stream);
-        if (st == BM_OK) st = dmalloc(&fresh[s].pid, (size_t)cap, stream);
+        bm_status_t st = dmalloc(&fresh[s].base, (size_t)N_PLANES * cap, stream, pool);
+        if (st == BM_OK) st = dmalloc(&fresh[s].pid, (size_t)cap, stream, pool);
         if (st != BM_OK) return st;
     }
     const ParticleSoA& old = h.dev.store[sel];
@@ -190,7 +207,7 @@ bm_status_t World::ensure_particle_capacity(SceneHost& h, int64_t need) {
     h.dev.store[1] = fresh[1];
     for (int32_t** p : {&h.dev.key, &h.dev.rank, &h.d_inv}) {
         if (*p) cudaFreeAsync(*p, stream);
-        bm_status_t st = dmalloc(p, (size_t)cap, stream);
+        bm_status_t st = dmalloc(p, (size_t)cap, stream, pool);
         if (st != BM_OK) return st;
     }
     dirty = true;
@@ -211,27 +228,23 @@ bm_status_t World::append_particles(SceneHost& h, int64_t n, const float* pos, c
     const int64_t n0 = h.n();
     bm_status_t st = ensure_particle_capacity(h, n0 + n);
     if (st != BM_OK) return st;
-    std::vector<float> buf((size_t)n * N_PLANES);
-    std::vector<int32_t> pid((size_t)n);
-    auto col = [&](int p) { return buf.data() + (size_t)p * n; };
-    for (int64_t q = 0; q < n; ++q) {
-        for (int a = 0; a < 3; ++a) {
-            col(P_X + a)[q] = pos[3 * q + a];
-            col(P_V + a)[q] = vel ? vel[3 * q + a] : 0.0f;
-        }
-        for (int a = 0; a < 9; ++a) {
-            col(P_F + a)[q] = (a % 4 == 0) ? 1.0f : 0.0f;
-            col(P_C + a)[q] = 0.0f;
-        }
-        const float m = mass ? mass[q] : 1.0f;
-        col(P_M)[q] = m;
-        col(P_V0)[q] = (h.density > 1e-12f) ? (m / h.density) : 1.0f;  // mpm_solver.h:30
-        pid[q] = (int32_t)(n0 + q);
-    }
-    ParticleSoA& s = h.dev.store[sel];
-    for (int p = 0; p < N_PLANES; ++p)
-        BM_CHECK_CUDA(cudaMemcpyAsync(s.plane(p) + n0, col(p), sizeof(float) * n, cudaMemcpyHostToDevice, stream));
-    BM_CHECK_CUDA(cudaMemcpyAsync(s.pid + n0, pid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
+    // only the caller's rows cross PCIe (28 B per particle); a kernel fills
+    // the remaining planes
+    float* rows = nullptr;
+    const size_t nf = (size_t)n * (vel ? 7 : 4);
+    st = dmalloc(&rows, nf, stream, pool);
+    if (st != BM_OK) return st;
+    float* d_pos = rows;
+    float* d_mass = rows + 3 * (size_t)n;
+    float* d_vel = vel ? rows + 4 * (size_t)n : nullptr;
+    BM_CHECK_CUDA(cudaMemcpyAsync(d_pos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+    if (mass) BM_CHECK_CUDA(cudaMemcpyAsync(d_mass, mass, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
+    if (vel) BM_CHECK_CUDA(cudaMemcpyAsync(d_vel, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+    launch_fill_particles(h.dev.store[sel], n0, n, d_pos, d_vel, mass ? d_mass : nullptr, h.density, stream);
+    cudaFreeAsync(rows, stream);
+    st = launch_status("append_particles");
+    if (st != BM_OK) return st;
+    // the caller may reuse its arrays when this returns (pinned ones too)
     BM_CHECK_CUDA(cudaStreamSynchronize(stream));
     h.dev.store[0].n = h.dev.store[1].n = n0 + n;
     update_bbox(h, n, pos);
@@ -260,18 +273,18 @@ bm_status_t World::ensure_grid(SceneHost& h) {
     if (nn <= 0 || nn > (int64_t)INT32_MAX / 2) return invalid_arg("grid box too large or empty");
     h.dev.g = g;
     for (auto& a : h.dev.acc) {
-        bm_status_t st = dmalloc(&a.mv, (size_t)nn, stream);
-        if (st == BM_OK) st = dmalloc(&a.f, (size_t)nn, stream);
-        if (st == BM_OK) st = dmalloc(&a.touched, (size_t)nb, stream);
-        if (st == BM_OK) st = dmalloc(&a.list, (size_t)nb, stream);
-        if (st == BM_OK) st = dmalloc(&a.count, 1, stream);
+        bm_status_t st = dmalloc(&a.mv, (size_t)nn, stream, pool);
+        if (st == BM_OK) st = dmalloc(&a.f, (size_t)nn, stream, pool);
+        if (st == BM_OK) st = dmalloc(&a.touched, (size_t)nb, stream, pool);
+        if (st == BM_OK) st = dmalloc(&a.list, (size_t)nb, stream, pool);
+        if (st == BM_OK) st = dmalloc(&a.count, 1, stream, pool);
         if (st != BM_OK) return st;
         BM_CHECK_CUDA(cudaMemsetAsync(a.mv, 0, sizeof(float4) * nn, stream));
         BM_CHECK_CUDA(cudaMemsetAsync(a.f, 0, sizeof(float4) * nn, stream));
         BM_CHECK_CUDA(cudaMemsetAsync(a.touched, 0, sizeof(uint32_t) * nb, stream));
         BM_CHECK_CUDA(cudaMemsetAsync(a.count, 0, sizeof(int32_t), stream));
     }
-    bm_status_t st = dmalloc(&h.dev.alloc, (size_t)nb, stream);
+    bm_status_t st = dmalloc(&h.dev.alloc, (size_t)nb, stream, pool);
     if (st != BM_OK) return st;
     BM_CHECK_CUDA(cudaMemsetAsync(h.dev.alloc, 0, (size_t)nb, stream));
     h.grid_ready = true;

@@ -54,6 +54,7 @@ public:
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;  // scene buffers (kept for reuse when freed)
     std::vector<SceneHost> scenes;
     int cur = 0;  // accumulation buffer of the current step
     int sel = 0;  // current particle store

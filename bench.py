@@ -7,7 +7,7 @@ Workload (default): the plain large rigid-wheel rut, 2,000,000 particles on a
 M1 coupler, G2P. Synthetic seeded inputs (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--forms plain,batched,served]
+                    [--forms plain,batched,served,adjoint]
 
 Beside the headline plain step the line carries the two other forms of the
 metric (one GPU only): "batched" (256 uneven box-drop scenes stepped
@@ -53,9 +53,9 @@ def parse():
                     help="SVD arithmetic of the fused step (default: the library default)")
     ap.add_argument("--sort-interval", type=int, default=None)
     ap.add_argument("--variant", type=int, default=None, help="launch shape of the fused kernel")
-    ap.add_argument("--forms", default="plain,batched,served",
+    ap.add_argument("--forms", default="plain,batched,served,adjoint",
                     help="comma list: plain (the headline wheel rut), batched (256 uneven scenes), "
-                         "served (Poisson request stream)")
+                         "served (Poisson request stream), adjoint (differentiable tine pass)")
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-rates", default="200,10", help="arrival rates (req/s) of the served runs")
@@ -321,7 +321,7 @@ def _host_body_step(body: dict, force, torque, gravity, dt):
     body["orientation"] = tuple(c / n for c in q) if n >= 1e-6 else (1.0, 0.0, 0.0, 0.0)
 
 
-def plain_scene_loop(scs, steps: int, warmup: int = 3):
+def plain_scene_loop(scs, steps, warmup: int = 3):
     """The plain per-scene loop: the scenes one after another through the
     drop-in solver API, each stepped `steps` times after `warmup` untimed
     steps. A dynamic body takes the reaction back to the host every step and
@@ -352,13 +352,13 @@ def plain_scene_loop(scs, steps: int, warmup: int = 3):
             one()
         s.sync()
         t0 = time.perf_counter()
-        for _ in range(steps):
+        for _ in range(sc.steps if steps is None else steps):
             one()
         st, _ = s.sync()
         secs += time.perf_counter() - t0
         if st != 0:
             raise RuntimeError(f"plain loop: scene {sc.name} reported status {st}")
-        work += sc.n * steps
+        work += sc.n * (sc.steps if steps is None else steps)
         s.close()
     return work / secs, work, secs
 
@@ -450,18 +450,62 @@ def run_served(args):
                      "server_p50_ms": st["p50_latency_ms"], "server_p99_ms": st["p99_latency_ms"],
                      "gpu_busy_rate": st["particle_steps"] / max(st["busy_seconds"], 1e-9),
                      "iterations": st["iterations"], "peak_bytes": st["peak_bytes"]})
-    loop_steps = 100
-    loop_rate, _, loop_secs = plain_scene_loop(all_reqs[:args.serve_requests], loop_steps)
+    # the first rate's requests, each for all of its steps, one after another
+    loop_rate, _, loop_secs = plain_scene_loop(all_reqs[:args.serve_requests], None)
     best = max(r["value"] for r in runs)
     return {"workload": "Poisson request stream: grid 32-128, 10k-1M particles (log-uniform, capped to fit "
                         "the grid), 100-2000 steps, friction angle 25-40 deg, half with a dynamic box or "
                         "cylinder; admission by a 150 GB HBM budget",
             "runs": runs, "value": best, "unit": UNIT,
-            "plain_loop": {"value": loop_rate, "unit": UNIT, "steps_per_request": loop_steps,
+            "plain_loop": {"value": loop_rate, "unit": UNIT, "steps_per_request": "all (100-2000)",
                            "seconds": loop_secs,
                            "what": "the first rate's requests one after another through the drop-in solver "
                                    "(host clock, body integrated on the host every step)"},
             "speedup_vs_plain_loop": best / loop_rate}
+
+
+def run_adjoint(args):
+    """Differentiable form: the tine pass (262,144 particles on the 64^3 grid,
+    200 steps at dt = 1e-4, 16 waypoints, checkpoints every 20 steps). The
+    forward records the run, the backward returns dL/d waypoint for the soft
+    heightfield loss. CUDA events on the solver stream around each pass (the
+    backward includes the upload of dL/dx and the download of the result)."""
+    import basements_b200 as bm
+    from basements_b200 import scenes
+
+    sc, body, wp, target = scenes.tine_pass()
+    s = bm.MPMSolver(sc.dx, domain=sc.domain)
+    s.set_material(sc.E, sc.nu, sc.rho)
+    s.set_plastic_alpha(sc.alpha)
+    s.add_particles(sc.position, None, sc.mass)
+    tape = bm.Tape(s, 20)
+    col = bm.make_collider(**body.as_tuple())
+    x0 = s.get_particles(("position", "velocity", "F", "C"))
+    fwd, bwd = [], []
+    for it in range(args.warmup + 3):
+        s.set_particles(0, position=x0["position"], velocity=x0["velocity"], F=x0["F"], C_=x0["C"])
+        s.sync()
+        s.timer_start()
+        tape.forward(sc.dt, sc.steps, col, wp)
+        f_ms = s.timer_stop()
+        L, g = scenes.heightfield_loss(s.get_particles()["position"], target)
+        s.timer_start()
+        gw = tape.backward(g)["dL_dwaypoints"]
+        b_ms = s.timer_stop()
+        if it >= args.warmup:
+            fwd.append(f_ms)
+            bwd.append(b_ms)
+    assert np.isfinite(gw).all()
+    f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
+    work = sc.n * sc.steps
+    tape.close()
+    s.close()
+    return {"workload": "tine pass: 262,144 particles, 64^3 grid, 200 steps at dt=1e-4, 16 waypoints, "
+                        "soft-heightfield L2 loss, checkpoints every 20 steps",
+            "forward_ms": f_ms, "backward_ms": b_ms, "loss": L,
+            "value": work / ((f_ms + b_ms) / 1e3), "unit": UNIT + " (forward + backward)",
+            "backward_over_forward": b_ms / f_ms, "timing": "CUDA events on the solver stream, median of 3",
+            "gradient_check": "tests/test_gpu_adjoint.py (FP64 central differences)"}
 
 
 def cpu_reference_rate(sc, n_steps: int, kind: str):
@@ -526,6 +570,8 @@ def main():
             out["batched"] = run_batched(args)
         if ranks.world == 1 and "served" in forms:
             out["served"] = run_served(args)
+        if ranks.world == 1 and "adjoint" in forms:
+            out["adjoint"] = run_adjoint(args)
         if ranks.rank == 0 and not args.no_cpu_baseline:
             from basements_b200 import scenes
             from oracle import oracle as O
