@@ -96,7 +96,8 @@ class ServerStats(C.Structure):
                 ("cancelled", C.c_int64), ("queued", C.c_int64), ("active", C.c_int64),
                 ("iterations", C.c_int64), ("p50_latency_ms", C.c_double), ("p99_latency_ms", C.c_double),
                 ("mean_latency_ms", C.c_double), ("particle_steps", C.c_double), ("busy_seconds", C.c_double),
-                ("peak_bytes", C.c_double)]
+                ("peak_bytes", C.c_double), ("admit_seconds", C.c_double), ("step_seconds", C.c_double),
+                ("retire_seconds", C.c_double)]
 
 
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = range(5)

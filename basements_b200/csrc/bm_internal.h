@@ -277,6 +277,9 @@ struct BodyDev {
 void launch_body_prepare(const SceneTable& t, const BodyDev* d_bodies, int n_bodies, M1Params* d_params,
                          cudaStream_t st);
 void launch_body_integrate(BodyDev* d_bodies, int n_bodies, const double* d_acc, cudaStream_t st);
+// out[k] = staged[k] with the state of old[src[k]] when src[k] >= 0.
+void launch_body_remap(const BodyDev* d_old, BodyDev* d_out, const BodyDev* d_staged, const int32_t* d_src, int n,
+                       cudaStream_t st);
 
 // Dense (i,j,k) copies of one scene's grid (plain API).
 void launch_grid_to_dense(const GridDesc& g, const GridAcc& a, const uint8_t* alloc, float* vel, float* force,

@@ -303,6 +303,25 @@ void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* 
     k_reaction_finalize<<<nblk(n_bodies, 64), 64, 0, st>>>(d_acc, n_bodies, d_out);
 }
 
+// The body array of the served form after its scene set changed: body k
+// takes its pose and velocities from old[src[k]] (a scene that stays) and
+// everything else from staged[k] (built on the host; its state is the initial
+// one for a new scene, src[k] < 0).
+__global__ void k_body_remap(const BodyDev* __restrict__ old, BodyDev* __restrict__ out,
+                             const BodyDev* __restrict__ staged, const int32_t* __restrict__ src, int n) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    BodyDev B = staged[k];
+    if (src[k] >= 0) B.state = old[src[k]].state;
+    out[k] = B;
+}
+
+void launch_body_remap(const BodyDev* d_old, BodyDev* d_out, const BodyDev* d_staged, const int32_t* d_src, int n,
+                       cudaStream_t st) {
+    if (n <= 0) return;
+    k_body_remap<<<nblk(n, 64), 64, 0, st>>>(d_old, d_out, d_staged, d_src, n);
+}
+
 void launch_body_prepare(const SceneTable& t, const BodyDev* d_bodies, int n_bodies, M1Params* d_params,
                          cudaStream_t st) {
     if (n_bodies <= 0) return;

@@ -5,16 +5,24 @@
 // estimated footprint fits the HBM budget (new scenes get their first P2G
 // while the running ones keep their precomputed one), step every co-resident
 // scene together (grid update, M1 + rigid update of every body, regrouping
-// when due, fused G2P + next P2G: one launch per phase for all scenes),
-// retire the scenes that have done their steps (particles and body copied to
-// host memory) and free their device memory. Latency is measured from submit
-// to the moment the result is on the host.
+// when due, fused G2P + next P2G: one launch per phase for all scenes), and
+// retire the scenes that have done their steps. Latency is measured from
+// submit to the moment the result is on the host.
+//
+// The worker never waits for the GPU while scenes are running: uploads go
+// on the World's upload stream, the scene table and the body arrays are
+// rebuilt in stream order (the bodies stay on the device and are remapped by
+// a kernel when the scene set changes), and a retired scene's particles and
+// body are read back into pinned memory behind an event; the request is
+// completed when its event has fired.
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -38,6 +46,11 @@ struct Request {
     bm_status_t error = BM_OK;
     bool cancel = false;
     Clock::time_point t_submit, t_done;
+    // read-back in flight: pinned block (x, v, F, C rows, status, body) and
+    // the event after its copies
+    void* pinned = nullptr;
+    size_t pinned_cap = 0;
+    cudaEvent_t ready = nullptr;
     // results
     std::vector<float> out_pos, out_vel, out_F, out_C;
     bm_collider_t out_body{};
@@ -46,6 +59,7 @@ struct Request {
 struct Active {
     std::shared_ptr<Request> req;
     int32_t steps_left = 0;
+    int body = -1;  // index in the device body arrays
 };
 
 double estimate_bytes(const bm_scene_desc_t& d) {
@@ -80,6 +94,19 @@ double percentile(std::vector<double> v, double q) {
     return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
 }
 
+size_t up16(size_t b) { return (b + 15) & ~size_t(15); }
+
+// Byte layout of a read-back block for n particles.
+struct Layout {
+    size_t rows, status, body, total;
+    explicit Layout(int64_t n) {
+        rows = 0;
+        status = up16(sizeof(float) * 24 * (size_t)n);
+        body = status + 16;
+        total = up16(body + sizeof(bm_collider_t));
+    }
+};
+
 }  // namespace
 
 struct bm_server {
@@ -87,18 +114,21 @@ struct bm_server {
     int device = 0;
     World w;
     std::vector<Active> active;  // same order as w.scenes
-    // bodies of the active scenes (rebuilt when the set changes)
-    std::vector<BodyDev> h_bodies;
+    // device bodies of the active scenes (pool memory, rebuilt in stream
+    // order when the scene set changes)
     BodyDev* d_bodies = nullptr;
     M1Params* d_params = nullptr;
     double* d_acc = nullptr;
     bm_reaction_t* d_react = nullptr;
-    int body_cap = 0;
     int64_t* d_cand_prefix = nullptr;  // body b owns M1 CTAs [prefix[b], prefix[b+1])
+    int n_bodies = 0;
     int64_t total_cand = 0;
-    float* h_stage = nullptr;  // pinned read-back staging of finished scenes
-    size_t stage_cap = 0;      // floats
     double used_bytes = 0;
+    // pinned read-back blocks and events, reused
+    std::multimap<size_t, void*> pinned_free;
+    std::vector<void*> pinned_all;
+    std::vector<cudaEvent_t> events_free;
+    std::vector<std::shared_ptr<Request>> draining;
     // shared state
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -111,75 +141,97 @@ struct bm_server {
     int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, iterations = 0, n_active = 0;
     std::vector<double> latencies;
     double particle_steps = 0, busy = 0, peak_bytes = 0;
+    double t_admit = 0, t_step = 0, t_retire = 0;
 };
 
 namespace {
 
-// Rebuilds the device body array from the active scenes, in scene order.
-// The current pose and velocities of each body are kept in its request
-// (save_bodies copies them back before the scene set changes).
-bm_status_t rebuild_bodies(bm_server* s) {
+template <class T>
+bm_status_t pool_alloc(bm_server* s, T** p, size_t count) {
+    *p = nullptr;
+    BM_CHECK_CUDA(cudaMallocFromPoolAsync((void**)p, sizeof(T) * std::max<size_t>(count, 1), s->w.pool, s->w.stream));
+    return BM_OK;
+}
+
+void pool_free(bm_server* s, void* p) {
+    if (p) cudaFreeAsync(p, s->w.stream);
+}
+
+// Rebuilds the device body arrays for the current active scenes. old_body[i]
+// is the index, in the arrays being replaced, of active scene i's body (-1:
+// a new scene, whose body starts from its request). Everything is enqueued
+// on the stream: no wait for the GPU.
+bm_status_t rebuild_bodies(bm_server* s, const std::vector<int>& old_body) {
     World& w = s->w;
-    std::vector<BodyDev> next;
+    std::vector<BodyDev> staged;
+    std::vector<int32_t> src;
     std::vector<int64_t> prefix(1, 0);
     for (size_t i = 0; i < s->active.size(); ++i) {
-        const Request& r = *s->active[i].req;
+        Active& a = s->active[i];
+        const Request& r = *a.req;
+        a.body = -1;
         if (!r.desc.has_body) continue;
         BodyDev B{};
-        B.state = r.out_body;
+        B.state = r.desc.body;
         B.inv_mass = r.desc.body.mass > 0.0f ? 1.0f / r.desc.body.mass : 0.0f;
         bool zero = true;
         for (int q = 0; q < 9; ++q) zero = zero && r.desc.body_inv_inertia[q] == 0.0f;
         for (int q = 0; q < 9; ++q)
             B.inv_inertia[q] = zero ? ((q % 4 == 0) ? 1.0f : 0.0f) : r.desc.body_inv_inertia[q];
-        for (int a = 0; a < 3; ++a) B.gravity[a] = r.desc.gravity[a];
+        for (int c = 0; c < 3; ++c) B.gravity[c] = r.desc.gravity[c];
         B.dt = r.desc.dt;
         B.dynamic = r.desc.body_dynamic;
         B.scene = (int32_t)i;
-        next.push_back(B);
+        a.body = (int)staged.size();
+        src.push_back(i < old_body.size() ? old_body[i] : -1);
+        staged.push_back(B);
         prefix.push_back(prefix.back() + m1_max_candidates(w.scenes[i].dev.g, r.desc.body.half_extents));
     }
-    s->h_bodies = next;
-    if ((int)next.size() > s->body_cap) {
-        cudaFree(s->d_bodies);
-        cudaFree(s->d_params);
-        cudaFree(s->d_acc);
-        cudaFree(s->d_react);
-        cudaFree(s->d_cand_prefix);
-        s->d_bodies = nullptr;
-        s->d_params = nullptr;
-        s->d_acc = nullptr;
-        s->d_react = nullptr;
-        s->d_cand_prefix = nullptr;
-        const int cap = std::max<int>((int)next.size(), s->body_cap * 2);
-        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_bodies, sizeof(BodyDev) * cap));
-        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_params, sizeof(M1Params) * cap));
-        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_acc, sizeof(double) * 7 * cap));
-        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_react, sizeof(bm_reaction_t) * cap));
-        BM_CHECK_CUDA(cudaMalloc((void**)&s->d_cand_prefix, sizeof(int64_t) * (cap + 1)));
-        s->body_cap = cap;
+    const int nb = (int)staged.size();
+    BodyDev* bodies = nullptr;
+    M1Params* params = nullptr;
+    double* acc = nullptr;
+    bm_reaction_t* react = nullptr;
+    int64_t* cand = nullptr;
+    bm_status_t st = BM_OK;
+    if (nb > 0) {
+        if ((st = pool_alloc(s, &bodies, nb)) != BM_OK) return st;
+        if ((st = pool_alloc(s, &params, nb)) != BM_OK) return st;
+        if ((st = pool_alloc(s, &acc, 7 * (size_t)nb)) != BM_OK) return st;
+        if ((st = pool_alloc(s, &react, nb)) != BM_OK) return st;
+        if ((st = pool_alloc(s, &cand, nb + 1)) != BM_OK) return st;
+        BodyDev* d_staged = nullptr;
+        int32_t* d_src = nullptr;
+        if ((st = pool_alloc(s, &d_staged, nb)) != BM_OK) return st;
+        if ((st = pool_alloc(s, &d_src, nb)) != BM_OK) return st;
+        const size_t b0 = up16(sizeof(BodyDev) * nb), b1 = up16(sizeof(int32_t) * nb), b2 = sizeof(int64_t) * (nb + 1);
+        void* buf = nullptr;
+        if ((st = w.stage_begin(b0 + b1 + b2, &buf)) != BM_OK) return st;
+        char* h = static_cast<char*>(buf);
+        std::memcpy(h, staged.data(), sizeof(BodyDev) * nb);
+        std::memcpy(h + b0, src.data(), sizeof(int32_t) * nb);
+        std::memcpy(h + b0 + b1, prefix.data(), b2);
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_staged, h, sizeof(BodyDev) * nb, cudaMemcpyHostToDevice, w.stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_src, h + b0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, w.stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(cand, h + b0 + b1, b2, cudaMemcpyHostToDevice, w.stream));
+        w.stage_done();
+        launch_body_remap(s->d_bodies, bodies, d_staged, d_src, nb, w.stream);
+        pool_free(s, d_staged);
+        pool_free(s, d_src);
     }
+    pool_free(s, s->d_bodies);
+    pool_free(s, s->d_params);
+    pool_free(s, s->d_acc);
+    pool_free(s, s->d_react);
+    pool_free(s, s->d_cand_prefix);
+    s->d_bodies = bodies;
+    s->d_params = params;
+    s->d_acc = acc;
+    s->d_react = react;
+    s->d_cand_prefix = cand;
+    s->n_bodies = nb;
     s->total_cand = prefix.back();
-    if (!next.empty()) {
-        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_bodies, next.data(), sizeof(BodyDev) * next.size(), cudaMemcpyHostToDevice,
-                                      w.stream));
-        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_cand_prefix, prefix.data(), sizeof(int64_t) * prefix.size(),
-                                      cudaMemcpyHostToDevice, w.stream));
-    }
-    BM_CHECK_CUDA(cudaStreamSynchronize(w.stream));
-    return BM_OK;
-}
-
-// Copies the device body states back into their requests (before the scene
-// set changes, so that rebuild_bodies starts from the current states).
-bm_status_t save_bodies(bm_server* s) {
-    if (s->h_bodies.empty()) return BM_OK;
-    std::vector<BodyDev> cur(s->h_bodies.size());
-    BM_CHECK_CUDA(cudaStreamSynchronize(s->w.stream));
-    BM_CHECK_CUDA(cudaMemcpy(cur.data(), s->d_bodies, sizeof(BodyDev) * cur.size(), cudaMemcpyDeviceToHost));
-    for (const BodyDev& b : cur)
-        if (b.scene >= 0 && b.scene < (int)s->active.size()) s->active[b.scene].req->out_body = b.state;
-    return BM_OK;
+    return launch_status("server bodies");
 }
 
 bm_status_t admit(bm_server* s, std::shared_ptr<Request> r) {
@@ -219,45 +271,110 @@ bm_status_t admit(bm_server* s, std::shared_ptr<Request> r) {
     return BM_OK;
 }
 
-// Copies a finished scene's particles (add order) and body to its request.
-bm_status_t collect(bm_server* s, int i) {
+bm_status_t pinned_acquire(bm_server* s, size_t bytes, void** out, size_t* cap) {
+    auto it = s->pinned_free.lower_bound(bytes);
+    if (it != s->pinned_free.end()) {
+        *cap = it->first;
+        *out = it->second;
+        s->pinned_free.erase(it);
+        return BM_OK;
+    }
+    size_t c = 1 << 16;
+    while (c < bytes) c <<= 1;
+    BM_CHECK_CUDA(cudaMallocHost(out, c));
+    s->pinned_all.push_back(*out);
+    *cap = c;
+    return BM_OK;
+}
+
+// Enqueues the read-back of active scene i (particles in add order, status
+// word, body) into a pinned block behind an event; the scene's device
+// memory may be freed right after (stream order).
+bm_status_t enqueue_collect(bm_server* s, int i) {
     World& w = s->w;
     SceneHost& h = w.scenes[i];
-    Request& r = *s->active[i].req;
+    Active& a = s->active[i];
+    Request& r = *a.req;
     const int64_t n = h.n();
-    r.out_pos.resize(3 * n);
-    r.out_vel.resize(3 * n);
-    r.out_F.resize(9 * n);
-    r.out_C.resize(9 * n);
-    // x, v, F, C rows land in pinned memory (a pageable read-back is several
-    // times slower and holds the worker while other scenes wait)
-    const size_t need = (size_t)24 * std::max<int64_t>(n, 1);
-    if (need > s->stage_cap) {
-        cudaFreeHost(s->h_stage);
-        s->h_stage = nullptr;
-        s->stage_cap = 0;
-        BM_CHECK_CUDA(cudaMallocHost((void**)&s->h_stage, sizeof(float) * need));
-        s->stage_cap = need;
-    }
-    struct Fld { std::vector<float>* dst; int plane; int width; size_t off; };
-    const Fld fs[] = {{&r.out_pos, P_X, 3, 0}, {&r.out_vel, P_V, 3, 3 * (size_t)n}, {&r.out_F, P_F, 9, 6 * (size_t)n},
-                      {&r.out_C, P_C, 9, 15 * (size_t)n}};
+    const Layout L(n);
+    bm_status_t st = pinned_acquire(s, L.total, &r.pinned, &r.pinned_cap);
+    if (st != BM_OK) return st;
+    char* base = static_cast<char*>(r.pinned);
     if (n > 0) {
         float* tmp = nullptr;
-        BM_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&tmp, sizeof(float) * 24 * n, w.pool, w.stream));
+        if ((st = pool_alloc(s, &tmp, 24 * (size_t)n)) != BM_OK) return st;
         const ParticleSoA& ps = h.dev.store[w.sel];
-        for (const Fld& f : fs) launch_gather_rows(ps, f.plane, f.width, tmp + f.off, w.stream);
-        BM_CHECK_CUDA(cudaMemcpyAsync(s->h_stage, tmp, sizeof(float) * 24 * n, cudaMemcpyDeviceToHost, w.stream));
-        cudaFreeAsync(tmp, w.stream);
+        const int planes[4] = {P_X, P_V, P_F, P_C}, widths[4] = {3, 3, 9, 9};
+        size_t off = 0;
+        for (int f = 0; f < 4; ++f) {
+            launch_gather_rows(ps, planes[f], widths[f], tmp + off, w.stream);
+            off += (size_t)widths[f] * n;
+        }
+        BM_CHECK_CUDA(cudaMemcpyAsync(base + L.rows, tmp, sizeof(float) * 24 * n, cudaMemcpyDeviceToHost, w.stream));
+        pool_free(s, tmp);
     }
-    uint32_t status = 0;
-    BM_CHECK_CUDA(cudaMemcpyAsync(&status, h.dev.status, sizeof(status), cudaMemcpyDeviceToHost, w.stream));
-    BM_CHECK_CUDA(cudaStreamSynchronize(w.stream));
-    if (n > 0)
-        for (const Fld& f : fs)
-            std::memcpy(f.dst->data(), s->h_stage + f.off, sizeof(float) * f.width * n);
-    r.error = (status & ERR_NONFINITE) ? BM_ERR_NON_FINITE : (status & ERR_ESCAPE) ? BM_ERR_DOMAIN_ESCAPE : BM_OK;
+    BM_CHECK_CUDA(cudaMemcpyAsync(base + L.status, h.dev.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, w.stream));
+    if (a.body >= 0)
+        BM_CHECK_CUDA(cudaMemcpyAsync(base + L.body, &s->d_bodies[a.body].state, sizeof(bm_collider_t),
+                                      cudaMemcpyDeviceToHost, w.stream));
+    else
+        std::memcpy(base + L.body, &r.out_body, sizeof(bm_collider_t));
+    if (s->events_free.empty()) {
+        cudaEvent_t e;
+        BM_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        s->events_free.push_back(e);
+    }
+    r.ready = s->events_free.back();
+    s->events_free.pop_back();
+    BM_CHECK_CUDA(cudaEventRecord(r.ready, w.stream));
     return BM_OK;
+}
+
+// Completes the requests whose read-back has arrived (all of them, waiting,
+// when `block`).
+void drain(bm_server* s, bool block) {
+    for (size_t k = 0; k < s->draining.size();) {
+        auto r = s->draining[k];
+        if (block) cudaEventSynchronize(r->ready);
+        else if (cudaEventQuery(r->ready) != cudaSuccess) {
+            ++k;
+            continue;
+        }
+        const int64_t n = (int64_t)r->mass.size();
+        const Layout L(n);
+        const char* base = static_cast<const char*>(r->pinned);
+        r->out_pos.resize(3 * n);
+        r->out_vel.resize(3 * n);
+        r->out_F.resize(9 * n);
+        r->out_C.resize(9 * n);
+        const float* rows = reinterpret_cast<const float*>(base + L.rows);
+        std::memcpy(r->out_pos.data(), rows, sizeof(float) * 3 * n);
+        std::memcpy(r->out_vel.data(), rows + 3 * n, sizeof(float) * 3 * n);
+        std::memcpy(r->out_F.data(), rows + 6 * n, sizeof(float) * 9 * n);
+        std::memcpy(r->out_C.data(), rows + 15 * n, sizeof(float) * 9 * n);
+        uint32_t status;
+        std::memcpy(&status, base + L.status, sizeof(status));
+        std::memcpy(&r->out_body, base + L.body, sizeof(bm_collider_t));
+        s->pinned_free.insert({r->pinned_cap, r->pinned});
+        r->pinned = nullptr;
+        s->events_free.push_back(r->ready);
+        r->ready = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->error = (status & ERR_NONFINITE) ? BM_ERR_NON_FINITE
+                       : (status & ERR_ESCAPE)  ? BM_ERR_DOMAIN_ESCAPE
+                                                : BM_OK;
+            r->t_done = Clock::now();
+            r->state = BM_REQ_DONE;
+            ++s->completed;
+            s->particle_steps += (double)n * r->n_steps;
+            s->latencies.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+            r->pos.clear();
+            r->vel.clear();
+        }
+        s->draining.erase(s->draining.begin() + k);
+        s->cv_done.notify_all();
+    }
 }
 
 bm_status_t step_all(bm_server* s, bool admitted) {
@@ -268,8 +385,8 @@ bm_status_t step_all(bm_server* s, bool admitted) {
     for (auto& h : w.scenes) any_fresh = any_fresh || h.dev.fresh;
     if (any_fresh) st = w.p2g_fresh();
     if (st == BM_OK) st = w.update(true);
-    if (st == BM_OK && !s->h_bodies.empty()) {
-        const int nb = (int)s->h_bodies.size();
+    if (st == BM_OK && s->n_bodies > 0) {
+        const int nb = s->n_bodies;
         BM_CHECK_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(double) * 7 * nb, w.stream));
         launch_body_prepare(w.table(), s->d_bodies, nb, s->d_params, w.stream);
         launch_m1_flat(w.table(), s->d_params, nb, s->d_cand_prefix, s->total_cand, w.cur, s->d_acc, w.stream);
@@ -287,11 +404,28 @@ bm_status_t step_all(bm_server* s, bool admitted) {
     return st;
 }
 
+void fail_request(bm_server* s, const std::shared_ptr<Request>& r, bm_status_t st) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->t_done = Clock::now();
+    if (r->cancel && st == BM_OK) {
+        r->state = BM_REQ_CANCELLED;
+        ++s->cancelled;
+    } else {
+        r->state = BM_REQ_FAILED;
+        r->error = st != BM_OK ? st : BM_ERR_CUDA;
+        ++s->failed;
+    }
+    r->pos.clear();
+    r->vel.clear();
+    s->cv_done.notify_all();
+}
+
 void worker_main(bm_server* s) {
     cudaSetDevice(s->device);
     World& w = s->w;
     for (;;) {
         std::vector<std::shared_ptr<Request>> to_admit;
+        if (s->active.empty() && !s->draining.empty()) drain(s, true);
         {
             std::unique_lock<std::mutex> lk(s->mu);
             while (!s->stop && s->queue.empty() && s->active.empty())
@@ -319,26 +453,34 @@ void worker_main(bm_server* s) {
             }
         }
         const auto t0 = Clock::now();
+        auto since = [](Clock::time_point a) { return std::chrono::duration<double>(Clock::now() - a).count(); };
+        double dt_admit = 0, dt_step = 0, dt_retire = 0;
         bool changed = false;
         if (!to_admit.empty()) {
-            save_bodies(s);
+            std::vector<int> old_body;
+            for (const Active& a : s->active) old_body.push_back(a.body);
             for (auto& r : to_admit) {
                 const bm_status_t st = admit(s, r);
-                if (st != BM_OK) {
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    r->state = BM_REQ_FAILED;
-                    r->error = st;
-                    r->t_done = Clock::now();
-                    ++s->failed;
-                    s->cv_done.notify_all();
-                }
+                if (st != BM_OK) fail_request(s, r, st);
+                else old_body.push_back(-1);
             }
             changed = true;
             s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
-            rebuild_bodies(s);
+            const bm_status_t st = rebuild_bodies(s, old_body);
+            if (st != BM_OK) {
+                for (auto& a : s->active) a.steps_left = 0;  // retire everything below as failed
+            }
+            dt_admit = since(t0);
         }
-        if (s->active.empty()) continue;
+        if (s->active.empty()) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->t_admit += dt_admit;
+            continue;
+        }
+        const auto t1 = Clock::now();
         bm_status_t st = step_all(s, changed);
+        dt_step = since(t1);
+        const auto t2 = Clock::now();
         {
             std::lock_guard<std::mutex> lk(s->mu);
             ++s->iterations;
@@ -351,44 +493,34 @@ void worker_main(bm_server* s) {
             if (st != BM_OK || a.steps_left <= 0 || a.req->cancel) done.push_back(i);
         }
         if (!done.empty()) {
-            save_bodies(s);
             for (int k = (int)done.size() - 1; k >= 0; --k) {
                 const int i = done[k];
                 auto r = s->active[i].req;
-                if (st == BM_OK && !r->cancel) collect(s, i);
-                {
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    r->t_done = Clock::now();
-                    if (st != BM_OK) {
-                        r->state = BM_REQ_FAILED;
-                        r->error = st;
-                        ++s->failed;
-                    } else if (r->cancel) {
-                        r->state = BM_REQ_CANCELLED;
-                        ++s->cancelled;
-                    } else {
-                        r->state = BM_REQ_DONE;
-                        ++s->completed;
-                        s->particle_steps += (double)r->mass.size() * r->n_steps;
-                        s->latencies.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
-                    }
-                    r->pos.clear();
-                    r->vel.clear();
-                }
+                bm_status_t cst = st;
+                if (cst == BM_OK && !r->cancel) cst = enqueue_collect(s, i);
+                if (cst == BM_OK && !r->cancel) s->draining.push_back(r);
+                else fail_request(s, r, cst);
                 s->used_bytes -= r->bytes;
                 w.remove_scene(i);
                 s->active.erase(s->active.begin() + i);
             }
-            rebuild_bodies(s);
-            s->cv_done.notify_all();
+            std::vector<int> old_body;
+            for (const Active& a : s->active) old_body.push_back(a.body);
+            rebuild_bodies(s, old_body);
         }
+        drain(s, false);
+        dt_retire = since(t2);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->busy += std::chrono::duration<double>(Clock::now() - t0).count();
+            s->t_admit += dt_admit;
+            s->t_step += dt_step;
+            s->t_retire += dt_retire;
             s->n_active = (int64_t)s->active.size();
         }
     }
-    // shutdown: cancel what is left
+    // shutdown: finish the read-backs in flight, cancel what is left
+    drain(s, true);
     std::lock_guard<std::mutex> lk(s->mu);
     for (auto& r : s->queue) r->state = BM_REQ_CANCELLED;
     for (auto& a : s->active) a.req->state = BM_REQ_CANCELLED;
@@ -440,13 +572,14 @@ BM_API bm_status_t bm_server_destroy(bm_server_t* s) {
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->device);
+    pool_free(s, s->d_bodies);
+    pool_free(s, s->d_params);
+    pool_free(s, s->d_acc);
+    pool_free(s, s->d_react);
+    pool_free(s, s->d_cand_prefix);
     s->w.release();
-    cudaFree(s->d_bodies);
-    cudaFree(s->d_params);
-    cudaFree(s->d_acc);
-    cudaFree(s->d_react);
-    cudaFree(s->d_cand_prefix);
-    cudaFreeHost(s->h_stage);
+    for (void* p : s->pinned_all) cudaFreeHost(p);
+    for (cudaEvent_t e : s->events_free) cudaEventDestroy(e);
     delete s;
     return BM_OK;
 }
@@ -578,6 +711,9 @@ BM_API bm_status_t bm_server_stats(bm_server_t* s, bm_server_stats_t* out) {
     r.particle_steps = s->particle_steps;
     r.busy_seconds = s->busy;
     r.peak_bytes = s->peak_bytes;
+    r.admit_seconds = s->t_admit;
+    r.step_seconds = s->t_step;
+    r.retire_seconds = s->t_retire;
     *out = r;
     return BM_OK;
 }

@@ -2,6 +2,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <cstring>
+
 #include "bm_world.h"
 
 namespace bm {
@@ -75,7 +77,30 @@ bm_status_t World::init() {
     BM_CHECK_CUDA(cudaMemPoolCreate(&pool, &props));
     uint64_t keep = UINT64_MAX;
     BM_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    BM_CHECK_CUDA(cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking));
+    BM_CHECK_CUDA(cudaEventCreateWithFlags(&upload_done, cudaEventDisableTiming));
+    for (auto& e : stage_used) BM_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return BM_OK;
+}
+
+bm_status_t World::stage_begin(size_t bytes, void** out) {
+    const int k = stage_next;
+    BM_CHECK_CUDA(cudaEventSynchronize(stage_used[k]));  // the copies that last read this buffer ran
+    if (stage_cap[k] < bytes) {
+        cudaFreeHost(stage_buf[k]);
+        stage_buf[k] = nullptr;
+        stage_cap[k] = 0;
+        const size_t cap = std::max<size_t>(bytes * 2, 1 << 16);
+        BM_CHECK_CUDA(cudaMallocHost(&stage_buf[k], cap));
+        stage_cap[k] = cap;
+    }
+    *out = stage_buf[k];
+    return BM_OK;
+}
+
+void World::stage_done() {
+    cudaEventRecord(stage_used[stage_next], stream);
+    stage_next ^= 1;
 }
 
 void World::free_scene(SceneHost& h) {
@@ -137,6 +162,18 @@ void World::release() {
     if (t1) cudaEventDestroy(t1);
     t0 = t1 = nullptr;
     if (stream) cudaStreamSynchronize(stream);
+    if (upload) cudaStreamSynchronize(upload);
+    for (int k = 0; k < 2; ++k) {
+        cudaFreeHost(stage_buf[k]);
+        stage_buf[k] = nullptr;
+        stage_cap[k] = 0;
+        if (stage_used[k]) cudaEventDestroy(stage_used[k]);
+        stage_used[k] = nullptr;
+    }
+    if (upload_done) cudaEventDestroy(upload_done);
+    upload_done = nullptr;
+    if (upload) cudaStreamDestroy(upload);
+    upload = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
     if (pool) cudaMemPoolDestroy(pool);
@@ -232,20 +269,23 @@ bm_status_t World::append_particles(SceneHost& h, int64_t n, const float* pos, c
     // the remaining planes
     float* rows = nullptr;
     const size_t nf = (size_t)n * (vel ? 7 : 4);
-    st = dmalloc(&rows, nf, stream, pool);
+    st = dmalloc(&rows, nf, upload, pool);
     if (st != BM_OK) return st;
     float* d_pos = rows;
     float* d_mass = rows + 3 * (size_t)n;
     float* d_vel = vel ? rows + 4 * (size_t)n : nullptr;
-    BM_CHECK_CUDA(cudaMemcpyAsync(d_pos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
-    if (mass) BM_CHECK_CUDA(cudaMemcpyAsync(d_mass, mass, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
-    if (vel) BM_CHECK_CUDA(cudaMemcpyAsync(d_vel, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+    BM_CHECK_CUDA(cudaMemcpyAsync(d_pos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, upload));
+    if (mass) BM_CHECK_CUDA(cudaMemcpyAsync(d_mass, mass, sizeof(float) * n, cudaMemcpyHostToDevice, upload));
+    if (vel) BM_CHECK_CUDA(cudaMemcpyAsync(d_vel, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, upload));
+    BM_CHECK_CUDA(cudaEventRecord(upload_done, upload));
+    BM_CHECK_CUDA(cudaStreamWaitEvent(stream, upload_done, 0));
     launch_fill_particles(h.dev.store[sel], n0, n, d_pos, d_vel, mass ? d_mass : nullptr, h.density, stream);
     cudaFreeAsync(rows, stream);
     st = launch_status("append_particles");
     if (st != BM_OK) return st;
-    // the caller may reuse its arrays when this returns (pinned ones too)
-    BM_CHECK_CUDA(cudaStreamSynchronize(stream));
+    // the caller may reuse its arrays when this returns, pinned ones too:
+    // wait for the copies only (not for the compute stream)
+    BM_CHECK_CUDA(cudaStreamSynchronize(upload));
     h.dev.store[0].n = h.dev.store[1].n = n0 + n;
     update_bbox(h, n, pos);
     dirty = true;
@@ -341,16 +381,26 @@ bm_status_t World::sync_table() {
     }
     sort.nkeys = keys;
     if (ns > 0) {
-        std::vector<FusedScene> views(ns);
+        // one pinned staging buffer: 4 view tables, the scene table, the prefix
+        auto up16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+        const size_t vb = up16(sizeof(FusedScene) * ns), sb = up16(sizeof(SceneDev) * ns),
+                     pb = sizeof(int64_t) * (ns + 1);
+        void* buf = nullptr;
+        bm_status_t st = stage_begin(4 * vb + sb + pb, &buf);
+        if (st != BM_OK) return st;
+        char* b = static_cast<char*>(buf);
         for (int c = 0; c < 2; ++c)
             for (int p = 0; p < 2; ++p) {
+                FusedScene* views = reinterpret_cast<FusedScene*>(b + (2 * c + p) * vb);
                 for (int q = 0; q < ns; ++q) views[q] = fused_view(host[q], c, p);
-                BM_CHECK_CUDA(cudaMemcpyAsync(d_views[c][p], views.data(), sizeof(FusedScene) * ns,
-                                              cudaMemcpyHostToDevice, stream));
+                BM_CHECK_CUDA(cudaMemcpyAsync(d_views[c][p], views, sizeof(FusedScene) * ns, cudaMemcpyHostToDevice,
+                                              stream));
             }
-        BM_CHECK_CUDA(cudaMemcpyAsync(d_scenes, host.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice, stream));
-        BM_CHECK_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice,
-                                      stream));
+        std::memcpy(b + 4 * vb, host.data(), sizeof(SceneDev) * ns);
+        std::memcpy(b + 4 * vb + sb, prefix.data(), pb);
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_scenes, b + 4 * vb, sizeof(SceneDev) * ns, cudaMemcpyHostToDevice, stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_prefix, b + 4 * vb + sb, pb, cudaMemcpyHostToDevice, stream));
+        stage_done();
     }
     dirty = false;
     return BM_OK;

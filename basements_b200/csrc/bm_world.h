@@ -55,6 +55,17 @@ public:
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;  // scene buffers (kept for reuse when freed)
+    // Host-to-device copies from pageable memory block their stream until all
+    // earlier work on it has run; particle uploads therefore go on their own
+    // stream, ordered before the compute stream's next kernel by an event.
+    cudaStream_t upload = nullptr;
+    cudaEvent_t upload_done = nullptr;
+    // Pinned, double-buffered staging for small uploads on `stream` (the scene
+    // table): a buffer is rewritten only after the copies that read it ran.
+    void* stage_buf[2] = {nullptr, nullptr};
+    size_t stage_cap[2] = {0, 0};
+    cudaEvent_t stage_used[2] = {nullptr, nullptr};
+    int stage_next = 0;
     std::vector<SceneHost> scenes;
     int cur = 0;  // accumulation buffer of the current step
     int sel = 0;  // current particle store
@@ -92,6 +103,11 @@ public:
     // P2G into acc[cur] of the scenes flagged `fresh` (their accumulators
     // are still zero), leaving the other scenes' precomputed P2G alone.
     bm_status_t p2g_fresh();
+
+    // A pinned buffer of at least `bytes` for copies enqueued on `stream`;
+    // stage_done() after enqueueing the copies that read it.
+    bm_status_t stage_begin(size_t bytes, void** out);
+    void stage_done();
 
     // Device table.
     bm_status_t sync_table();

@@ -324,6 +324,10 @@ typedef struct bm_server_stats {
     double particle_steps;     /* of completed requests */
     double busy_seconds;       /* wall time with scenes on the device */
     double peak_bytes;         /* largest admitted footprint */
+    /* host time of the worker's phases: admitting requests (upload, grid,
+     * bodies), enqueueing the batched steps, retiring finished requests
+     * (read-back, release) */
+    double admit_seconds, step_seconds, retire_seconds;
 } bm_server_stats_t;
 
 BM_API bm_status_t bm_server_create(const bm_server_config_t* config, bm_server_t** out);
