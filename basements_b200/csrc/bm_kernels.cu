@@ -301,24 +301,30 @@ __global__ void __launch_bounds__(kParticleCTA) k_g2p(SceneTable t, int cur, int
 __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, int64_t EYZ, int64_t EZ,
                                               const float wgt[3][3], const float dcs[3][3], float v[3],
                                               float Cm[9]) {
+    // separable in k: per (i, j) row, s = sum_k w_k v_k and t = sum_k w_k dk v_k,
+    // then v += w_ij s and C += w_ij (di s, dj s, t)
+    const float wd2[3] = {wgt[2][0] * dcs[2][0], wgt[2][1] * dcs[2][1], wgt[2][2] * dcs[2][2]};
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const float4* row = src + i * EYZ + j * EZ;
             const float4 n[3] = {row[0], row[1], row[2]};
+            const float sx = (n[0].x * wgt[2][0] + n[1].x * wgt[2][1]) + n[2].x * wgt[2][2];
+            const float sy = (n[0].y * wgt[2][0] + n[1].y * wgt[2][1]) + n[2].y * wgt[2][2];
+            const float sz = (n[0].z * wgt[2][0] + n[1].z * wgt[2][1]) + n[2].z * wgt[2][2];
+            const float tx = (n[0].x * wd2[0] + n[1].x * wd2[1]) + n[2].x * wd2[2];
+            const float ty = (n[0].y * wd2[0] + n[1].y * wd2[1]) + n[2].y * wd2[2];
+            const float tz = (n[0].z * wd2[0] + n[1].z * wd2[1]) + n[2].z * wd2[2];
             const float wij = wgt[0][i] * wgt[1][j];
+            const float wi0 = wij * dcs[0][i], wj1 = wij * dcs[1][j];
+            const float sv[3] = {sx, sy, sz}, tv[3] = {tx, ty, tz};
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float w = wij * wgt[2][k];
-                const float wv[3] = {n[k].x * w, n[k].y * w, n[k].z * w};
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    v[a] += wv[a];
-                    Cm[3 * a + 0] += wv[a] * dcs[0][i];
-                    Cm[3 * a + 1] += wv[a] * dcs[1][j];
-                    Cm[3 * a + 2] += wv[a] * dcs[2][k];
-                }
+            for (int a = 0; a < 3; ++a) {
+                v[a] += wij * sv[a];
+                Cm[3 * a + 0] += wi0 * sv[a];
+                Cm[3 * a + 1] += wj1 * sv[a];
+                Cm[3 * a + 2] += wij * tv[a];
             }
         }
 }
