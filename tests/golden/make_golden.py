@@ -7,7 +7,8 @@ built reference harness (``make -C oracle``):
 
 Every array is produced either by the reference's OWN code (oracle/_ref,
 compiled from the reference headers) or read from the reference's shipped
-research outputs (box_drop_M1.csv). Nothing here runs at test time; the tests
+research outputs (box_drop_M1.csv, and the M1 rows of box_drop_dense, tine_drag
+and rover_wheel). Nothing here runs at test time; the tests
 only read the .npz files, so they also run where the reference is absent.
 """
 from __future__ import annotations
@@ -37,6 +38,21 @@ def box_drop_csv(ref_root: str):
         m = list(csv.reader(f))
     metrics = {k: float(v) for k, v in zip(m[0][1:], m[1][1:])}
     return cols, data, metrics
+
+
+def research_csv(ref_root: str, scene: str, summary: str):
+    """One scene's M1 time series and its summary row, as the reference's
+    research bench wrote them (research/mpm_rigid_coupling/bench_compare_all.cpp:
+    box_drop_dense :505-613, tine_drag :215-292, rover_wheel :614-800)."""
+    base = os.path.join(ref_root, "research/mpm_rigid_coupling/outputs/csv")
+    with open(os.path.join(base, f"{scene}_M1.csv")) as f:
+        rows = list(csv.reader(f))
+    data = np.array([[float(v) for v in r] for r in rows[1:]], np.float64)
+    with open(os.path.join(base, f"{scene}_M1_{summary}.csv")) as f:
+        m = list(csv.reader(f))
+    return {f"{scene}_columns": np.array(rows[0]), f"{scene}_rows": data,
+            f"{scene}_metric_names": np.array(m[0][1:]),
+            f"{scene}_metric_values": np.array([float(v) for v in m[1][1:]])}
 
 
 def small_scene(seed=3, cells=(8, 4, 8), ppc=4):
@@ -184,6 +200,10 @@ def main():
     np.savez_compressed(os.path.join(HERE, "box_drop_M1.npz"), columns=np.array(cols), rows=data,
                         metric_names=np.array(list(metrics)), metric_values=np.array(list(metrics.values())),
                         ref_rows=O.box_drop_m1("ref"))
+    scenes_m1 = {}
+    for scene, summary in (("box_drop_dense", "metrics"), ("tine_drag", "summary"), ("rover_wheel", "metrics")):
+        scenes_m1.update(research_csv(a.ref_root, scene, summary))
+    np.savez_compressed(os.path.join(HERE, "m1_scenes.npz"), **scenes_m1)
     np.savez_compressed(os.path.join(HERE, "small_scene.npz"), **run_small_scene())
     np.savez_compressed(os.path.join(HERE, "m1_cases.npz"), **m1_cases())
     np.savez_compressed(os.path.join(HERE, "svd_cases.npz"), **svd_cases())

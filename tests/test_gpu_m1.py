@@ -5,8 +5,8 @@
   dt = 0): grid after the call and nodes_inside exactly, force and torque to
   1e-5 relative (the reference sums in float in hash-map order, the kernel in
   double per CTA);
-* the reference's grid-only box_drop scene (research harness, 720 steps)
-  against its shipped CSV;
+* the reference's grid-only research scenes (box_drop, box_drop_dense,
+  tine_drag, rover_wheel; 480-720 steps) against their shipped CSVs;
 * a particle scene with a cylinder through bm_solver_step_coupled against the
   reference's split phases P2G -> update_grid -> apply -> G2P.
 """
@@ -114,6 +114,42 @@ def test_box_drop_scene_matches_reference_csv():
     names = list(gold["metric_names"])
     max_p = np.abs(rows[:, 6]).max()
     assert abs(max_p - gold["metric_values"][names.index("max_abs_total_p_y")]) < 1e-4 * 0.18
+
+
+@pytest.mark.parametrize("scene", ["box_drop_dense", "tine_drag", "rover_wheel"])
+def test_research_scenes_match_reference_csv(scene):
+    """The other grid-only M1 research scenes (bench_compare_all.cpp:
+    box_drop_dense :505-613, tine_drag :215-292, rover_wheel :614-800): the
+    float32 harness loop of tests/m1_scene_loop.py around the CUDA coupler,
+    against the reference's shipped CSVs. The same loop around the float
+    restatement reproduces those CSVs to their 7 printed digits (CPU test), so
+    what is left here is the coupler's reaction sum (double per CTA against
+    the reference's float sum in hash-map order) carried through the scene."""
+    from tests import m1_scene_loop as L
+    gold = np.load(os.path.join(GOLD, "m1_scenes.npz"))
+    ref = gold[scene + "_rows"]
+    vals = dict(zip(gold[scene + "_metric_names"], gold[scene + "_metric_values"]))
+    rows = L.run(scene, L.GpuGrid(bm, L.SCENES[scene]))
+    if scene == "tine_drag":
+        fx, fy, n = L.tine_summary(rows)
+        sub = rows[::4]
+        print(f"tine_drag: max |dFx| = {np.abs(sub[:, 2] - ref[:, 2]).max():.3e} N, "
+              f"avg draft {fx:.6f} N (reference {vals['avg_draft_fx_n']:.6f})")
+        np.testing.assert_allclose(sub[:, 1], ref[:, 1], rtol=2e-6, atol=1e-6)
+        np.testing.assert_allclose(sub[:, 2:], ref[:, 2:], rtol=1e-5, atol=1e-5)
+        assert n == vals["samples"]
+        assert abs(fx - vals["avg_draft_fx_n"]) <= 1e-5 * abs(vals["avg_draft_fx_n"])
+        return
+    e_pos = np.abs(rows[:, 1:4] - ref[:, 1:4]).max()
+    e_vy = np.abs(rows[:, 4] - ref[:, 4]).max()
+    max_p = np.abs(rows[:, 7]).max()
+    print(f"{scene}: max |dx| = {e_pos:.3e} m, max |dvy| = {e_vy:.3e} m/s, first row off by 1e-5: "
+          f"{L.first_divergence(rows[:, 1:4], ref[:, 1:4], 1e-5)}, max |sum p_y| {max_p:.6f} "
+          f"(reference {vals['max_abs_total_p_y']:.6f})")
+    assert e_pos <= 2e-5
+    assert e_vy <= 2e-4
+    assert np.array_equal(rows[:, 9], ref[:, 9])
+    assert abs(max_p - vals["max_abs_total_p_y"]) <= 1e-4 * vals["max_abs_total_p_y"]
 
 
 def test_coupled_particle_scene_matches_reference_split():

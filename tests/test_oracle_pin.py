@@ -105,6 +105,32 @@ def test_box_drop_reproduces_reference_csv():
     assert abs(np.abs(p_sum).mean() - d["metric_values"][names.index("avg_abs_total_p_y")]) < 1e-6
 
 
+@pytest.mark.parametrize("scene", ["box_drop_dense", "tine_drag", "rover_wheel"])
+def test_m1_research_scenes_reproduce_reference_csv(scene):
+    """The remaining grid-only M1 research scenes (bench_compare_all.cpp:
+    box_drop_dense :505-613, tine_drag :215-292, rover_wheel :614-800), run by
+    the float32 harness loop around the float restatement of the coupler,
+    against the reference's shipped CSVs (7 significant digits; t to 4-6 decimals)."""
+    from tests import m1_scene_loop as L
+    d = load("m1_scenes.npz")
+    ref = d[scene + "_rows"]
+    rows = L.run(scene, L.OracleGrid(O, "f32", L.SCENES[scene]))
+    vals = dict(zip(d[scene + "_metric_names"], d[scene + "_metric_values"]))
+    if scene == "tine_drag":
+        rows = rows[::4]  # the bench logs every 4th step
+        assert rows.shape == ref.shape
+        np.testing.assert_allclose(rows[:, 1:], ref[:, 1:], rtol=2e-6, atol=1e-6)
+        fx, fy, n = L.tine_summary(L.run(scene, L.OracleGrid(O, "f32", L.SCENES[scene])))
+        assert n == vals["samples"]
+        assert abs(fx - vals["avg_draft_fx_n"]) <= 2e-6 * abs(vals["avg_draft_fx_n"])
+        assert abs(fy - vals["avg_vertical_fy_n"]) <= 1e-6
+        return
+    assert rows.shape == ref.shape
+    np.testing.assert_allclose(rows[:, 1:8], ref[:, 1:8], rtol=2e-6, atol=1e-6)
+    assert np.array_equal(rows[:, 9], ref[:, 9])
+    assert abs(np.abs(rows[:, 7]).max() - vals["max_abs_total_p_y"]) <= 2e-6 * vals["max_abs_total_p_y"]
+
+
 @pytest.mark.skipif(not O.available("ref"), reason="reference harness oracle/_ref not built")
 def test_live_bit_exact_vs_compiled_reference():
     sc = scenes.sand_column()
