@@ -7,8 +7,9 @@ built reference harness (``make -C oracle``):
 
 Every array is produced either by the reference's OWN code (oracle/_ref,
 compiled from the reference headers) or read from the reference's shipped
-research outputs (box_drop_M1.csv, and the M1 rows of box_drop_dense, tine_drag
-and rover_wheel). Nothing here runs at test time; the tests
+research outputs (box_drop_M1.csv, and the M1 rows of box_drop_dense, tine_drag,
+rover_wheel and foot_step, the M1 run of the rigid-drift benchmark, and the
+repose-pile summary). Nothing here runs at test time; the tests
 only read the .npz files, so they also run where the reference is absent.
 """
 from __future__ import annotations
@@ -40,19 +41,45 @@ def box_drop_csv(ref_root: str):
     return cols, data, metrics
 
 
-def research_csv(ref_root: str, scene: str, summary: str):
-    """One scene's M1 time series and its summary row, as the reference's
+def research_csv(ref_root: str, scene: str, summaries):
+    """One scene's M1 time series and its summary rows, as the reference's
     research bench wrote them (research/mpm_rigid_coupling/bench_compare_all.cpp:
-    box_drop_dense :505-613, tine_drag :215-292, rover_wheel :614-800)."""
+    tine_drag :215-292, foot_step :374-504, box_drop_dense :505-613,
+    rover_wheel :614-800)."""
     base = os.path.join(ref_root, "research/mpm_rigid_coupling/outputs/csv")
     with open(os.path.join(base, f"{scene}_M1.csv")) as f:
         rows = list(csv.reader(f))
     data = np.array([[float(v) for v in r] for r in rows[1:]], np.float64)
-    with open(os.path.join(base, f"{scene}_M1_{summary}.csv")) as f:
-        m = list(csv.reader(f))
+    names, values = [], []
+    for summary in summaries:
+        with open(os.path.join(base, f"{scene}_M1_{summary}.csv")) as f:
+            m = list(csv.reader(f))
+        names += m[0][1:]
+        values += [float(v) for v in m[1][1:]]
     return {f"{scene}_columns": np.array(rows[0]), f"{scene}_rows": data,
-            f"{scene}_metric_names": np.array(m[0][1:]),
-            f"{scene}_metric_values": np.array([float(v) for v in m[1][1:]])}
+            f"{scene}_metric_names": np.array(names), f"{scene}_metric_values": np.array(values)}
+
+
+def drift_pic_csv(ref_root: str):
+    """benchmarks/bench_mpm_rigid_drift.cpp --method pic (:24-178): a unit box
+    dropped on a 5x3x5 grid patch through M1; its shipped time series."""
+    with open(os.path.join(ref_root, "outputs/figures/mpm_rigid_drift_pic.csv")) as f:
+        rows = list(csv.reader(f))
+    return {"rigid_drift_columns": np.array(rows[0]),
+            "rigid_drift_rows": np.array([[float(v) for v in r] for r in rows[1:]], np.float64)}
+
+
+def repose_summary(ref_root: str):
+    """research/mpm_rigid_coupling/outputs/csv/repose_pile_summary.csv
+    (bench_compare_all.cpp:293-371): the settled pile of the particle run."""
+    with open(os.path.join(ref_root, "research/mpm_rigid_coupling/outputs/csv/repose_pile_summary.csv")) as f:
+        m = list(csv.reader(f))
+    names = m[0][:-1]  # the last column is the literature range as text
+    return {"metric_names": np.array(names), "metric_values": np.array([float(v) for v in m[1][:-1]])}
+
+
+M1_SCENES = (("box_drop_dense", ("metrics",)), ("tine_drag", ("summary",)), ("rover_wheel", ("metrics", "roll")),
+             ("foot_step", ("metrics", "rebound")))
 
 
 def small_scene(seed=3, cells=(8, 4, 8), ppc=4):
@@ -201,9 +228,11 @@ def main():
                         metric_names=np.array(list(metrics)), metric_values=np.array(list(metrics.values())),
                         ref_rows=O.box_drop_m1("ref"))
     scenes_m1 = {}
-    for scene, summary in (("box_drop_dense", "metrics"), ("tine_drag", "summary"), ("rover_wheel", "metrics")):
-        scenes_m1.update(research_csv(a.ref_root, scene, summary))
+    for scene, summaries in M1_SCENES:
+        scenes_m1.update(research_csv(a.ref_root, scene, summaries))
+    scenes_m1.update(drift_pic_csv(a.ref_root))
     np.savez_compressed(os.path.join(HERE, "m1_scenes.npz"), **scenes_m1)
+    np.savez_compressed(os.path.join(HERE, "repose_pile.npz"), **repose_summary(a.ref_root))
     np.savez_compressed(os.path.join(HERE, "small_scene.npz"), **run_small_scene())
     np.savez_compressed(os.path.join(HERE, "m1_cases.npz"), **m1_cases())
     np.savez_compressed(os.path.join(HERE, "svd_cases.npz"), **svd_cases())

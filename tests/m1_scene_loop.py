@@ -3,7 +3,8 @@ coupler that exposes ``apply``/``grid`` access (the CUDA solver or the oracle).
 
 The loop restates research/mpm_rigid_coupling/bench_compare_all.cpp in float32:
 
-* box_drop_dense (:505-613) and rover_wheel (:614-800): a dynamic body; each
+* foot_step (:374-504), box_drop_dense (:505-613) and rover_wheel (:614-800):
+  a dynamic body; each
   step applies gravity to the body, calls the coupler, adds its reaction,
   integrates with the reference's semi-implicit Euler
   (include/basements/physics/dynamics/integrator.h:20-45, damping 0 as the
@@ -11,10 +12,13 @@ The loop restates research/mpm_rigid_coupling/bench_compare_all.cpp in float32:
   make_wheel leave it), then adds grid gravity and the floor clamp to every
   node with mass;
 * tine_drag (:215-292): a kinematic box moved by v*dt before each call; the
-  reaction is only measured.
+  reaction is only measured;
+* rigid_drift: benchmarks/bench_mpm_rigid_drift.cpp --method pic (:24-178),
+  the same dynamic loop over a smaller patch.
 
 Scenario constants follow research/mpm_rigid_coupling/scenarios/
-scenario_box_drop.h, scenario_tine_drag.h and scenario_rover_wheel.h.
+scenario_box_drop.h, scenario_foot_step.h, scenario_tine_drag.h and
+scenario_rover_wheel.h.
 """
 from __future__ import annotations
 
@@ -53,6 +57,16 @@ SCENES = {
                            domain=((-8, -4, -8), (16, 16, 16)), center=(0.0, 0.55, 0.0),
                            half=(0.2, 0.2, 0.2), q=(1.0, 0.0, 0.0, 0.0), vel=(0, 0, 0), omg=(0, 0, 0),
                            friction=0.5, mass=9.0, shape=0, steps=720, kinematic=False),
+    # scenario_foot_step.h: a thin dynamic box stamped onto a 7x3x7 patch
+    "foot_step": dict(dx=0.1, seed_lo=(-3, 0, -3), seed_hi=(3, 2, 3), node_mass=0.01,
+                      domain=((-8, -4, -8), (16, 16, 16)), center=(0.0, 0.55, 0.0),
+                      half=(0.10, 0.02, 0.10), q=(1.0, 0.0, 0.0, 0.0), vel=(0, 0, 0), omg=(0, 0, 0),
+                      friction=0.5, mass=1.0, shape=0, steps=480, kinematic=False),
+    # benchmarks/bench_mpm_rigid_drift.cpp:37-69: the unit box over a 5x3x5 patch
+    "rigid_drift": dict(dx=0.1, seed_lo=(-2, 0, -2), seed_hi=(2, 2, 2), node_mass=0.01,
+                        domain=((-8, -4, -8), (16, 16, 16)), center=(0.0, 0.55, 0.0),
+                        half=(0.2, 0.2, 0.2), q=(1.0, 0.0, 0.0, 0.0), vel=(0, 0, 0), omg=(0, 0, 0),
+                        friction=0.5, mass=1.0, shape=0, steps=720, kinematic=False),
     # scenario_tine_drag.h: surface_y = (4 - 1 + 0.5) dx, tip 6 cm below it
     "tine_drag": dict(dx=0.05, seed_lo=(-2, 0, -3), seed_hi=(10, 3, 3), node_mass=0.1875,
                       domain=((-8, -4, -8), (24, 16, 16)), center=None, half=(0.005, 0.05, 0.04),
@@ -163,6 +177,29 @@ def tine_summary(rows, start=0.5):
     """Average draft -Fx and vertical Fy over t > start (bench_compare_all.cpp:259-275)."""
     sel = rows[:, 0].astype(np.float32) > f32(start)
     return -rows[sel, 2].mean(), rows[sel, 3].mean(), int(sel.sum())
+
+
+def rebound(rows, settle=0.05):
+    """ReboundTracker (scenario_foot_step.h:84-113) over the body's v_y:
+    returns (v_down_peak, v_up_peak)."""
+    state, down, up = 0, f32(0), f32(0)
+    for t, vy in zip(rows[:, 0].astype(np.float32), rows[:, 4].astype(np.float32)):
+        if t < f32(settle):
+            continue
+        if state == 0:
+            down = min(down, vy)
+            if vy >= 0 and down < 0:
+                state = 1
+        if state == 1:
+            up = max(up, vy)
+            if vy <= 0 and up > 0:
+                state = 2
+    return float(down), float(up)
+
+
+# rigid_drift CSV columns [t, box_y, box_vy, p_body_y, p_grid_y, p_sum_y, KE_box,
+# nodes_inside] as columns of the dynamic rows above
+DRIFT_COLUMNS = [0, 2, 4, 5, 6, 7, 8, 9]
 
 
 def first_divergence(a, b, atol):

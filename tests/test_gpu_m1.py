@@ -6,7 +6,9 @@
   1e-5 relative (the reference sums in float in hash-map order, the kernel in
   double per CTA);
 * the reference's grid-only research scenes (box_drop, box_drop_dense,
-  tine_drag, rover_wheel; 480-720 steps) against their shipped CSVs;
+  foot_step, tine_drag, rover_wheel; 480-720 steps) and the rigid-drift
+  benchmark's M1 run against their shipped CSVs;
+* the reference's cylinder inside-test KATs, probed through the coupler;
 * a particle scene with a cylinder through bm_solver_step_coupled against the
   reference's split phases P2G -> update_grid -> apply -> G2P.
 """
@@ -116,10 +118,11 @@ def test_box_drop_scene_matches_reference_csv():
     assert abs(max_p - gold["metric_values"][names.index("max_abs_total_p_y")]) < 1e-4 * 0.18
 
 
-@pytest.mark.parametrize("scene", ["box_drop_dense", "tine_drag", "rover_wheel"])
+@pytest.mark.parametrize("scene", ["box_drop_dense", "foot_step", "tine_drag", "rover_wheel"])
 def test_research_scenes_match_reference_csv(scene):
     """The other grid-only M1 research scenes (bench_compare_all.cpp:
-    box_drop_dense :505-613, tine_drag :215-292, rover_wheel :614-800): the
+    tine_drag :215-292, foot_step :374-504, box_drop_dense :505-613,
+    rover_wheel :614-800): the
     float32 harness loop of tests/m1_scene_loop.py around the CUDA coupler,
     against the reference's shipped CSVs. The same loop around the float
     restatement reproduces those CSVs to their 7 printed digits (CPU test), so
@@ -150,6 +153,36 @@ def test_research_scenes_match_reference_csv(scene):
     assert e_vy <= 2e-4
     assert np.array_equal(rows[:, 9], ref[:, 9])
     assert abs(max_p - vals["max_abs_total_p_y"]) <= 1e-4 * vals["max_abs_total_p_y"]
+    if scene == "foot_step":
+        down, up = L.rebound(rows)
+        assert abs(down - vals["v_down_peak"]) <= 1e-4 * abs(vals["v_down_peak"]) and up == vals["v_up_peak"]
+
+
+def test_rigid_drift_pic_matches_reference_csv():
+    """benchmarks/bench_mpm_rigid_drift.cpp --method pic: the unit box over a
+    5x3x5 patch, 720 steps, against outputs/figures/mpm_rigid_drift_pic.csv."""
+    from tests import m1_scene_loop as L
+    ref = np.load(os.path.join(GOLD, "m1_scenes.npz"))["rigid_drift_rows"]
+    rows = L.run("rigid_drift", L.GpuGrid(bm, L.SCENES["rigid_drift"]))[:, L.DRIFT_COLUMNS]
+    e_y = np.abs(rows[:, 1] - ref[:, 1]).max()
+    e_vy = np.abs(rows[:, 2] - ref[:, 2]).max()
+    print(f"rigid_drift: max |dy| = {e_y:.3e} m, max |dvy| = {e_vy:.3e} m/s")
+    assert e_y <= 2e-5 and e_vy <= 2e-4
+    assert np.array_equal(rows[:, 7], ref[:, 7])
+    np.testing.assert_allclose(rows[:, 5], ref[:, 5], atol=1e-4 * np.abs(ref[:, 5]).max())
+
+
+def test_cylinder_inside_kats():
+    """tests/test_mpm_rigid_cylinder.cpp:37-255 through the CUDA M1: the
+    inside-test cases, and the 200-probe rolling sweep entering and leaving
+    once, probe for probe equal to the oracle's M1."""
+    from tests import shape_kats as K
+    for name, point, q, expect in K.KATS:
+        assert K.probe_gpu(bm, point, q) == expect, name
+    probes = K.rolling_probes()
+    seq = [K.probe_gpu(bm, p, q) for p, q in probes]
+    assert K.transitions(seq) == 2
+    assert seq == [K.probe_oracle(O, REF, p, q) for p, q in probes]
 
 
 def test_coupled_particle_scene_matches_reference_split():

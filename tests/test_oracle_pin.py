@@ -105,10 +105,11 @@ def test_box_drop_reproduces_reference_csv():
     assert abs(np.abs(p_sum).mean() - d["metric_values"][names.index("avg_abs_total_p_y")]) < 1e-6
 
 
-@pytest.mark.parametrize("scene", ["box_drop_dense", "tine_drag", "rover_wheel"])
+@pytest.mark.parametrize("scene", ["box_drop_dense", "foot_step", "tine_drag", "rover_wheel"])
 def test_m1_research_scenes_reproduce_reference_csv(scene):
     """The remaining grid-only M1 research scenes (bench_compare_all.cpp:
-    box_drop_dense :505-613, tine_drag :215-292, rover_wheel :614-800), run by
+    tine_drag :215-292, foot_step :374-504, box_drop_dense :505-613,
+    rover_wheel :614-800), run by
     the float32 harness loop around the float restatement of the coupler,
     against the reference's shipped CSVs (7 significant digits; t to 4-6 decimals)."""
     from tests import m1_scene_loop as L
@@ -129,6 +130,59 @@ def test_m1_research_scenes_reproduce_reference_csv(scene):
     np.testing.assert_allclose(rows[:, 1:8], ref[:, 1:8], rtol=2e-6, atol=1e-6)
     assert np.array_equal(rows[:, 9], ref[:, 9])
     assert abs(np.abs(rows[:, 7]).max() - vals["max_abs_total_p_y"]) <= 2e-6 * vals["max_abs_total_p_y"]
+    if scene == "foot_step":
+        down, up = L.rebound(rows)
+        assert abs(down - vals["v_down_peak"]) <= 2e-6 * abs(vals["v_down_peak"]) and up == vals["v_up_peak"]
+
+
+def test_rigid_drift_pic_reproduces_reference_csv():
+    """outputs/figures/mpm_rigid_drift_pic.csv, written by
+    benchmarks/bench_mpm_rigid_drift.cpp --method pic (9 printed digits)."""
+    from tests import m1_scene_loop as L
+    ref = load("m1_scenes.npz")["rigid_drift_rows"]
+    rows = L.run("rigid_drift", L.OracleGrid(O, "f32", L.SCENES["rigid_drift"]))[:, L.DRIFT_COLUMNS]
+    assert rows.shape == ref.shape
+    np.testing.assert_allclose(rows[:, 1:7], ref[:, 1:7], rtol=2e-8, atol=1e-9)
+    assert np.array_equal(rows[:, 7], ref[:, 7])
+
+
+def test_repose_pile_reproduces_reference_summary():
+    """research/mpm_rigid_coupling/outputs/csv/repose_pile_summary.csv: 245
+    particles, 1920 steps. The run is chaotic (the reference rebuilt here
+    lands 0.0024 deg from its shipped geometric angle), so the summary is
+    pinned to 0.1 deg and 2e-4 relative, the particles at rest exactly."""
+    from tests import repose_pile as RP
+    d = load("repose_pile.npz")
+    ref = dict(zip(d["metric_names"], d["metric_values"]))
+    pos, m = RP.column()
+    M = RP.MATERIAL
+    s = O.CpuSolver("f32", RP.DX)
+    s.set_material(M["E"], M["nu"], M["rho"])
+    s.set_plastic_alpha(M["alpha"])
+    s.set_floor_friction(M["floor_friction"])
+    s.add_particles(pos, None, m)
+    s.step(RP.DT, RP.STEPS)
+    p = s.get_particles()
+    got = RP.measure_pile(p["position"], p["velocity"])
+    assert len(pos) == ref["particle_count"]
+    assert abs(got["angle_geom"] - ref["angle_geom_deg"]) < 0.1
+    assert abs(got["angle_slope"] - ref["angle_slope_deg"]) < 0.1
+    assert abs(got["height"] - ref["settled_height_m"]) < 2e-4 * ref["settled_height_m"]
+    assert abs(got["radius"] - ref["settled_radius_m"]) < 2e-4 * ref["settled_radius_m"]
+    assert got["at_rest"] == ref["particles_at_rest"]
+
+
+@pytest.mark.parametrize("kind", ["f32", "ref"])
+def test_cylinder_inside_kats_through_m1(kind):
+    """tests/test_mpm_rigid_cylinder.cpp:37-255 (inside-test cases and the
+    rolling monotonicity sweep), probed through the oracle's M1."""
+    if kind == "ref" and not O.available("ref"):
+        pytest.skip("reference harness oracle/_ref not built")
+    from tests import shape_kats as K
+    for name, point, q, expect in K.KATS:
+        assert K.probe_oracle(O, kind, point, q) == expect, name
+    seq = [K.probe_oracle(O, kind, p, q) for p, q in K.rolling_probes()]
+    assert K.transitions(seq) == 2
 
 
 @pytest.mark.skipif(not O.available("ref"), reason="reference harness oracle/_ref not built")
