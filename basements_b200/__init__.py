@@ -144,6 +144,7 @@ _SIGS = {
     "bm_solver_seed_grid": (_st, [_h, C.c_int64, _i32, _f, _f]),
     "bm_solver_set_grid_velocity": (_st, [_h, _f]),
     "bm_solver_sync": (_st, [_h, C.POINTER(C.c_int64)]),
+    "bm_solver_light_node_suspects": (_st, [_h, C.POINTER(C.c_int64)]),
     "bm_solver_stream": (_st, [_h, C.POINTER(C.c_void_p)]),
     "bm_solver_profile_enable": (_st, [_h, C.c_int32]),
     "bm_solver_profile_read": (_st, [_h, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
@@ -159,6 +160,7 @@ _SIGS = {
     "bm_batch_get_body": (_st, [_h, C.c_int32, C.POINTER(Collider)]),
     "bm_batch_get_reaction": (_st, [_h, C.c_int32, C.POINTER(Reaction)]),
     "bm_batch_sync": (_st, [_h, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "bm_batch_light_node_suspects": (_st, [_h, C.POINTER(C.c_int64)]),
     "bm_batch_set_graph": (_st, [_h, C.c_int32]),
     "bm_batch_set_launch": (_st, [_h, C.c_int32, C.c_int32, C.c_int32]),
     "bm_batch_autotune": (_st, [_h, C.c_int32, C.POINTER(TuneResult)]),
@@ -411,6 +413,14 @@ class MPMSolver:
         st = lib().bm_solver_sync(self._h, C.byref(esc))
         return st, esc.value
 
+    def light_node_suspects(self) -> int:
+        """Nodes whose particle mass fell from >= 1e-4 to (0, 1e-6] in one step
+        (the only places the fused step can depart from the reference's
+        momentum-without-force rule); 0 means none so far."""
+        n = C.c_int64()
+        check(lib().bm_solver_light_node_suspects(self._h, C.byref(n)), "bm_solver_light_node_suspects")
+        return n.value
+
     def profile(self, on=True):
         check(lib().bm_solver_profile_enable(self._h, 1 if on else 0), "bm_solver_profile_enable")
 
@@ -522,6 +532,11 @@ class Batch:
         esc = C.c_int64()
         st = lib().bm_batch_sync(self._h, C.byref(bad), C.byref(esc))
         return st, bad.value, esc.value
+
+    def light_node_suspects(self) -> int:
+        n = C.c_int64()
+        check(lib().bm_batch_light_node_suspects(self._h, C.byref(n)), "bm_batch_light_node_suspects")
+        return n.value
 
     def set_graph(self, on: bool):
         check(lib().bm_batch_set_graph(self._h, 1 if on else 0), "bm_batch_set_graph")

@@ -438,6 +438,20 @@ BM_API bm_status_t bm_batch_get_reaction(bm_batch_t* b, int32_t scene, bm_reacti
     return BM_OK;
 }
 
+BM_API bm_status_t bm_batch_light_node_suspects(bm_batch_t* b, int64_t* out) {
+    if (!b || !out) return invalid_arg("NULL argument");
+    DeviceGuard dg(b->w.device);
+    BM_CHECK_CUDA(cudaStreamSynchronize(b->w.stream));
+    int64_t total = 0;
+    for (SceneHost& h : b->w.scenes) {
+        unsigned long long n = 0;
+        BM_CHECK_CUDA(cudaMemcpy(&n, h.dev.escaped + 1, sizeof(n), cudaMemcpyDeviceToHost));
+        total += (int64_t)n;
+    }
+    *out = total;
+    return BM_OK;
+}
+
 BM_API bm_status_t bm_batch_sync(bm_batch_t* b, int32_t* bad_scene, int64_t* escaped) {
     if (!b) return invalid_arg("NULL handle");
     DeviceGuard dg(b->w.device);

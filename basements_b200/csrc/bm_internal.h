@@ -17,6 +17,18 @@ namespace bm {
 // Device-side error bits, OR-ed into a scene's status word.
 enum : uint32_t { ERR_ESCAPE = 1u, ERR_NONFINITE = 2u };
 
+// Node mass (particle contributions only) from which a node counts as heavy
+// for the light-contribution rule of the fused kernel: 100x the reference's
+// 1e-6 threshold of update_grid (mpm_solver.h:257).
+constexpr float kHeavyNodeMass = 1e-4f;
+
+// Total mass of a node after the couplers of this step: the coupler keeps the
+// particle mass in mv.w and writes the node's new total into f.w (0 until a
+// coupler touches the node).
+__host__ __device__ __forceinline__ float node_total_mass(const float4& mv, const float4& f) {
+    return f.w != 0.0f ? f.w : mv.w;
+}
+
 // Threads per CTA of every per-particle kernel except the fused one (the
 // CTA -> scene prefix table is built for this size; the fused kernel's
 // variants use multiples of it).
@@ -119,7 +131,7 @@ struct SceneDev {
     int32_t bin_shift;     // sort bins are 2^bin_shift nodes per axis (0: one cell)
     int32_t fresh;         // 1: acc[cur] holds a standalone (unfolded) P2G this step
     uint32_t* status;      // error bits
-    unsigned long long* escaped;  // dropped stencil writes
+    unsigned long long* escaped;  // [0] dropped stencil writes, [1] light-node suspects (k_grid_update)
 };
 
 struct SceneTable {

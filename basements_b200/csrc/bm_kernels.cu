@@ -150,6 +150,12 @@ __global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int
 // update_grid over the blocks listed in acc[cur] of scene blockIdx.y (every
 // other node of the box is empty, so skipping it is exact); the same launch
 // zeroes the blocks listed in acc[1-cur] so that it can take the next P2G.
+// Before zeroing a node of acc[1-cur] (the previous step's grid, particle
+// mass in .w) it counts the node as a light-node suspect when that mass was
+// at least kHeavyNodeMass and the node's new particle mass in a folded
+// acc[cur] is in (0, 1e-6]: only there can the fused kernel have skipped a
+// force record that update_grid needs (the mass lane of acc[cur] is not
+// changed by this launch).
 __global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int cur, bool folded_all) {
     const SceneDev& S = t.scenes[blockIdx.y];
     const bool folded = folded_all && !S.fresh;
@@ -164,6 +170,10 @@ __global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int 
         if (slot >= n_cur) {
             const int64_t b = o.list[slot - n_cur];
             const int64_t id = g.node_of_block(b, tt);
+            if (folded && o.mv[id].w >= kHeavyNodeMass) {
+                const float m_new = c.mv[id].w;
+                if (m_new > 0.0f && m_new <= 1e-6f) atomicAdd(S.escaped + 1, 1ull);
+            }
             o.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
             o.f[id] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (tt == 0) o.touched[b] = 0u;
@@ -300,9 +310,10 @@ __global__ void __launch_bounds__(kParticleCTA) k_g2p(SceneTable t, int cur, int
 // multiplies instead of skipping, which is the same for finite grid values.
 __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, int64_t EYZ, int64_t EZ,
                                               const float wgt[3][3], const float dcs[3][3], float v[3],
-                                              float Cm[9]) {
+                                              float Cm[9], uint32_t& heavy) {
     // separable in k: per (i, j) row, s = sum_k w_k v_k and t = sum_k w_k dk v_k,
-    // then v += w_ij s and C += w_ij (di s, dj s, t)
+    // then v += w_ij s and C += w_ij (di s, dj s, t); bit 9i+3j+k of heavy is
+    // set when that node's particle mass is at least kHeavyNodeMass
     const float wd2[3] = {wgt[2][0] * dcs[2][0], wgt[2][1] * dcs[2][1], wgt[2][2] * dcs[2][2]};
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -310,6 +321,8 @@ __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, in
         for (int j = 0; j < 3; ++j) {
             const float4* row = src + i * EYZ + j * EZ;
             const float4 n[3] = {row[0], row[1], row[2]};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) heavy |= (n[k].w >= kHeavyNodeMass ? 1u : 0u) << (9 * i + 3 * j + k);
             const float sx = (n[0].x * wgt[2][0] + n[1].x * wgt[2][1]) + n[2].x * wgt[2][2];
             const float sy = (n[0].y * wgt[2][0] + n[1].y * wgt[2][1]) + n[2].y * wgt[2][2];
             const float sz = (n[0].z * wgt[2][0] + n[1].z * wgt[2][1]) + n[2].z * wgt[2][2];
@@ -334,8 +347,13 @@ __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, in
 // (momentum + force * dt, mass), the force folded in with the scene's dt. The
 // reference keeps momentum without force at nodes of mass <= 1e-6
 // (mpm_solver.h:257); every contribution to such a node has w*m <= 1e-6 on
-// its own, so exactly those contributions also add their force to the force
-// channel, and the grid update subtracts force * dt again there. A particle
+// its own, so those light contributions also add their force to the force
+// channel, and the grid update subtracts force * dt again there. A light
+// contribution skips that record when its node held at least kHeavyNodeMass
+// of particle mass in this step's grid and the particle's base node did not
+// change (the node is then in both stencils); a node can only end light with
+// a record missing if its mass fell from >= kHeavyNodeMass to <= 1e-6 in one
+// step, and the grid update counts every such node (light-node suspects). A particle
 // whose 3x3x3 stencil lies inside the box (all but escaping particles)
 // addresses its nodes at constant offsets from the base node with one bounds
 // check for the whole stencil, and its affine and stress terms are summed
@@ -368,6 +386,8 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
     float Cm[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) Cm[q] = 0.0f;
+    uint32_t heavy = 0u;
+    const int gbase0 = base[0], gbase1 = base[1], gbase2 = base[2];
     {
         const float4* __restrict__ cur_mv = S.cur_mv;
         const float cs = 4.0f * g.inv_dx * g.inv_dx;
@@ -381,7 +401,7 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
             for (int a = 0; a < 3; ++a)
 #pragma unroll
                 for (int i = 0; i < 3; ++i) dcs[a][i] = dd[a][i] * cs;
-            gather_inside(cur_mv + g.node_rel(r0, r1, r2), EYZ, EZ, wgt, dcs, v, Cm);
+            gather_inside(cur_mv + g.node_rel(r0, r1, r2), EYZ, EZ, wgt, dcs, v, Cm, heavy);
         } else {
 #pragma unroll 1
             for (int n = 0; n < 27; ++n) {
@@ -443,6 +463,7 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
 #pragma unroll
         for (int i = 0; i < 3; ++i) dd[a][i] = ((float)(base[a] + i) - fx[a] - 0.5f) * g.dx;
     }
+    if (base[0] != gbase0 || base[1] != gbase1 || base[2] != gbase2) heavy = 0u;
     {
         const int r0 = base[0] - g.ox, r1 = base[1] - g.oy, r2 = base[2] - g.oz;
         const bool inside = (unsigned)r0 <= (unsigned)(g.ex() - 3) && (unsigned)r1 <= (unsigned)(g.ey() - 3) &&
@@ -481,7 +502,8 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
                         red_v4(dmv + off, (qj[0] + Cm[2] * dd[2][k]) * mc + s0 * wdt,
                                (qj[1] + Cm[5] * dd[2][k]) * mc + s1 * wdt, (qj[2] + Cm[8] * dd[2][k]) * mc + s2 * wdt,
                                mc);
-                        if (mc <= 1e-6f) red_v4(df + off, s0 * w, s1 * w, s2 * w, 0.0f);
+                        if (mc <= 1e-6f && !(heavy & (1u << (9 * i + 3 * j + k))))
+                            red_v4(df + off, s0 * w, s1 * w, s2 * w, 0.0f);
                     }
                 }
             }

@@ -118,23 +118,31 @@ __global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params,
         const int64_t id = g.node_of_block(blin, tt);
         float r[3], vb[3];
         if (m1_node_inside(P, dx, ox + li, oy + lj, oz + lk, r, vb)) {
+            // the node's mass is its particle mass (mv.w) plus what couplers
+            // added this step; the new total goes to f.w, mv.w keeps the
+            // particle mass (the fused kernel's light-contribution rule reads it)
             float4 nv = A.mv[id];
+            float4 nf = A.f[id];
+            const float m_tot = node_total_mass(nv, nf);
             float va[3];
-            if (!(nv.w >= 1e-9f)) {  // inactive (mass 0) or mass < 1e-9: body claims the node
+            if (!(m_tot >= 1e-9f)) {  // inactive (mass 0) or mass < 1e-9: body claims the node
                 va[0] = vb[0]; va[1] = vb[1]; va[2] = vb[2];
-                nv = make_float4(vb[0], vb[1], vb[2], P.mb);
+                nv = make_float4(vb[0], vb[1], vb[2], 0.0f);
+                nf.w = P.mb;
             } else {
-                const float mn = add(nv.w, P.mb);
-                const float pa[3] = {add(mul(nv.x, nv.w), mul(vb[0], P.mb)), add(mul(nv.y, nv.w), mul(vb[1], P.mb)),
-                                     add(mul(nv.z, nv.w), mul(vb[2], P.mb))};
+                const float mn = add(m_tot, P.mb);
+                const float pa[3] = {add(mul(nv.x, m_tot), mul(vb[0], P.mb)), add(mul(nv.y, m_tot), mul(vb[1], P.mb)),
+                                     add(mul(nv.z, m_tot), mul(vb[2], P.mb))};
                 if (fabsf(mn) < 1e-6f) {  // Vec3 division guard of the reference
                     va[0] = va[1] = va[2] = 0.0f;
                 } else {
                     va[0] = dvd(pa[0], mn); va[1] = dvd(pa[1], mn); va[2] = dvd(pa[2], mn);
                 }
-                nv = make_float4(va[0], va[1], va[2], mn);
+                nv = make_float4(va[0], va[1], va[2], nv.w);
+                nf.w = mn;
             }
             A.mv[id] = nv;
+            A.f[id] = nf;
             touch_block(A, blin);
             const float dF[3] = {mul(sub(va[0], vb[0]), P.mb_over_dt), mul(sub(va[1], vb[1]), P.mb_over_dt),
                                  mul(sub(va[2], vb[2]), P.mb_over_dt)};
@@ -232,13 +240,12 @@ __global__ void k_grid_to_dense(GridDesc g, GridAcc a, const uint8_t* alloc, flo
     const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.num_nodes()) return;  // the flat layout is the dense (i,j,k) order
     const float4 mv = a.mv[q];
+    const float4 f = a.f[q];
+    const float m = node_total_mass(mv, f);
     if (vel) { vel[3 * q] = mv.x; vel[3 * q + 1] = mv.y; vel[3 * q + 2] = mv.z; }
-    if (force) {
-        const float4 f = a.f[q];
-        force[3 * q] = f.x; force[3 * q + 1] = f.y; force[3 * q + 2] = f.z;
-    }
-    if (mass) mass[q] = mv.w;
-    if (active) active[q] = mv.w > 0.0f ? 1 : 0;
+    if (force) { force[3 * q] = f.x; force[3 * q + 1] = f.y; force[3 * q + 2] = f.z; }
+    if (mass) mass[q] = m;
+    if (active) active[q] = m > 0.0f ? 1 : 0;
     if (balloc) balloc[q] = alloc[g.block_of_node(q)];
 }
 
@@ -248,7 +255,8 @@ __global__ void k_dense_velocity_to_grid(GridDesc g, GridAcc a, const float* vel
     float4 mv = a.mv[q];
     mv.x = vel[3 * q]; mv.y = vel[3 * q + 1]; mv.z = vel[3 * q + 2];
     a.mv[q] = mv;
-    if (mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f || mv.w != 0.0f) touch_block(a, g.block_of_node(q));
+    if (mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f || node_total_mass(mv, a.f[q]) != 0.0f)
+        touch_block(a, g.block_of_node(q));
 }
 
 __global__ void k_seed(GridDesc g, GridAcc a, uint8_t* alloc, int64_t n, const int32_t* ijk, const float* vel,
@@ -261,6 +269,7 @@ __global__ void k_seed(GridDesc g, GridAcc a, uint8_t* alloc, int64_t n, const i
         return;
     }
     a.mv[id] = make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], mass[q]);
+    a.f[id].w = 0.0f;  // the seeded mass is the node's whole mass
     const int64_t b = g.block_of_node(id);
     alloc[b] = 1;
     touch_block(a, b);

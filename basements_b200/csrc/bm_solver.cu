@@ -585,6 +585,16 @@ BM_API bm_status_t bm_solver_set_grid_velocity(bm_solver_t* s, const float* vel)
     return st;
 }
 
+BM_API bm_status_t bm_solver_light_node_suspects(bm_solver_t* s, int64_t* out) {
+    if (!s || !out) return invalid_arg("NULL argument");
+    DeviceGuard dg(s->w.device);
+    unsigned long long n = 0;
+    BM_CHECK_CUDA(cudaMemcpyAsync(&n, s->sc().dev.escaped + 1, sizeof(n), cudaMemcpyDeviceToHost, s->w.stream));
+    BM_CHECK_CUDA(cudaStreamSynchronize(s->w.stream));
+    *out = (int64_t)n;
+    return BM_OK;
+}
+
 BM_API bm_status_t bm_solver_sync(bm_solver_t* s, int64_t* escaped) {
     if (!s) return invalid_arg("NULL handle");
     DeviceGuard dg(s->w.device);

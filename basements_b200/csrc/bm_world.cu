@@ -195,9 +195,9 @@ bm_status_t World::p2g_fresh() {
 int World::add_scene() {
     scenes.emplace_back();
     SceneHost& h = scenes.back();
-    if (dmalloc(&h.dev.status, 1, stream, pool) == BM_OK && dmalloc(&h.dev.escaped, 1, stream, pool) == BM_OK) {
+    if (dmalloc(&h.dev.status, 1, stream, pool) == BM_OK && dmalloc(&h.dev.escaped, 2, stream, pool) == BM_OK) {
         cudaMemsetAsync(h.dev.status, 0, sizeof(uint32_t), stream);
-        cudaMemsetAsync(h.dev.escaped, 0, sizeof(unsigned long long), stream);
+        cudaMemsetAsync(h.dev.escaped, 0, 2 * sizeof(unsigned long long), stream);
     }
     dirty = true;
     return (int)scenes.size() - 1;

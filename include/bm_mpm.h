@@ -218,6 +218,14 @@ BM_API bm_status_t bm_solver_set_grid_velocity(bm_solver_t* s, const float* velo
  * clears it. escaped (may be NULL) gets the number of stencil writes dropped
  * because they fell outside the box. */
 BM_API bm_status_t bm_solver_sync(bm_solver_t* s, int64_t* escaped);
+/* Nodes, counted since the handle was created, whose particle mass fell from
+ * at least 1e-4 to (0, 1e-6] in one step. update_grid (mpm_solver.h:257)
+ * keeps the momentum without force at nodes of mass <= 1e-6; the fused
+ * kernel records the force of a light contribution except at nodes that held
+ * at least 1e-4 in the previous step's grid, so only these nodes can miss a
+ * record. 0 means every step so far kept the reference's rule exactly. No
+ * counterpart in the reference. */
+BM_API bm_status_t bm_solver_light_node_suspects(bm_solver_t* s, int64_t* out);
 /* The CUDA stream (cudaStream_t) the handle enqueues on. */
 BM_API bm_status_t bm_solver_stream(bm_solver_t* s, void** stream);
 /* Per-kernel timing with CUDA events on the handle's stream (off by default).
@@ -282,6 +290,8 @@ BM_API bm_status_t bm_batch_get_body(bm_batch_t* b, int32_t scene, bm_collider_t
 BM_API bm_status_t bm_batch_get_reaction(bm_batch_t* b, int32_t scene, bm_reaction_t* out);
 /* Waits; returns the first device-side error of any scene (and which). */
 BM_API bm_status_t bm_batch_sync(bm_batch_t* b, int32_t* bad_scene, int64_t* escaped);
+/* bm_solver_light_node_suspects summed over the batch's scenes. */
+BM_API bm_status_t bm_batch_light_node_suspects(bm_batch_t* b, int64_t* out);
 BM_API bm_status_t bm_batch_set_graph(bm_batch_t* b, int32_t on);
 BM_API bm_status_t bm_batch_set_launch(bm_batch_t* b, int32_t variant, int32_t sort_interval, int32_t bin_shift);
 /* Times each candidate launch setting for `trial_steps` steps on this batch

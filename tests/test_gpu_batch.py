@@ -31,6 +31,7 @@ def test_batch_matches_reference_scene_by_scene():
     steps = 40
     b.step(steps)
     assert b.sync()[0] == 0
+    assert b.light_node_suspects() == 0
     for i, sc in enumerate(scs):
         c = O.CpuSolver(REF, sc.dx)
         c.set_material(sc.E, sc.nu, sc.rho)

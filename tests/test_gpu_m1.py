@@ -203,6 +203,7 @@ def test_coupled_particle_scene_matches_reference_split():
     print(f"coupled wheel scene, 40 steps: max |x_gpu - x_ref| = {e:.3e} dx")
     assert e <= POS_TOL_100
     assert g.sync() == (0, 0)
+    assert g.light_node_suspects() == 0
 
 
 def test_overlapping_bodies_apply_in_order_like_the_reference():

@@ -95,6 +95,28 @@ def test_sand_column_100_and_1000_steps(fast_math):
     print(f"sand column 1000 steps: max |x_gpu - x_ref| = {e1000:.3e} dx")
     assert e1000 <= POS_TOL_1000
     assert g.sync() == (0, 0)
+    assert g.light_node_suspects() == 0
+
+
+def test_light_node_suspect_is_counted_and_stays_within_the_bar():
+    """One heavy particle (1e-3 kg, no gravity, no stress) crosses 0.96 of its
+    base cell in one step: the node behind it goes from 2.7e-4 kg to 1.1e-7 kg
+    of mass, so the fused step skipped that light contribution's force record
+    (the node was heavy in the gathered grid) and the grid update counts the
+    node. The particle carries no stress, so the missing record is zero and
+    the run still equals the reference."""
+    dx, dt = 1.0 / 32.0, 1e-3
+    v = 0.96 * dx / dt
+    pos = np.array([[(10 + 0.02 + 0.5) * dx, 11.0 * dx, 11.0 * dx]], np.float32)
+    vel = np.array([[v, 0.0, 0.0]], np.float32)
+    mass = np.array([1e-3], np.float32)
+    g = gpu_solver(dx, pos, vel, mass, gravity=(0.0, 0.0, 0.0), domain=((0, 0, 0), (64, 32, 32)))
+    c = cpu_solver(REF, dx, pos, vel, mass, gravity=(0.0, 0.0, 0.0))
+    g.step(dt, 3)
+    c.step(dt, 3)
+    assert g.sync() == (0, 0)
+    assert g.light_node_suspects() >= 1
+    assert max_err_dx(g.get_particles()["position"], c.get_particles()["position"], dx) <= POS_TOL_100
 
 
 def test_two_runs_agree_within_atomic_order_bound():
