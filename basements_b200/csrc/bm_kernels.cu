@@ -342,6 +342,45 @@ __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, in
         }
 }
 
+// mark_stencil_blocks for particles in base-node order: a lane whose block
+// range equals that of the lane before it leaves the marks to that lane, and
+// the allocated flags are skipped when alloc_done (the blocks of a stencil the
+// particle gathered from in full were allocated by its own scatter, or the
+// lane that covered it, one step earlier).
+__device__ __forceinline__ void mark_stencil_blocks_warp(const GridDesc& g, const GridAcc& a, uint8_t* alloc,
+                                                         const int base[3], const float wx[3], const float wy[3],
+                                                         const float wz[3], bool alloc_done) {
+    const int lo0 = base[0] + (wx[0] == 0.0f), hi0 = base[0] + 2 - (wx[2] == 0.0f);
+    const int lo1 = base[1] + (wy[0] == 0.0f), hi1 = base[1] + 2 - (wy[2] == 0.0f);
+    const int lo2 = base[2] + (wz[0] == 0.0f), hi2 = base[2] + 2 - (wz[2] == 0.0f);
+    const int b0 = (lo0 - g.ox) >> 2, b1 = (lo1 - g.oy) >> 2, b2 = (lo2 - g.oz) >> 2;
+    const int e0 = ((hi0 - g.ox) >> 2) - b0, e1 = ((hi1 - g.oy) >> 2) - b1, e2 = ((hi2 - g.oz) >> 2) - b2;
+    const int lane = (int)(threadIdx.x & 31);
+    // a 3-node stencil covers one or two blocks per axis (e in {0, 1}); block
+    // indices far outside the box (a non-finite position) get a key of their
+    // own so that they never stand in for another lane
+    const bool near_box = (unsigned)(b0 + 1) <= (unsigned)(g.nbx + 1) && (unsigned)(b1 + 1) <= (unsigned)(g.nby + 1) &&
+                          (unsigned)(b2 + 1) <= (unsigned)(g.nbz + 1);
+    const unsigned long long key = near_box ? ((unsigned long long)(b0 & 0xFFFFF) << 43) |
+                                                  ((unsigned long long)(b1 & 0xFFFFF) << 23) |
+                                                  ((unsigned long long)(b2 & 0xFFFFF) << 3) |
+                                                  (unsigned)(e0 << 2 | e1 << 1 | e2)
+                                            : ~0ull - (unsigned long long)lane;
+    const unsigned act = __activemask();
+    const unsigned long long prev = __shfl_up_sync(act, key, 1);
+    const bool covered = lane > 0 && ((act >> (lane - 1)) & 1u) && prev == key;
+    if (covered) return;
+    for (int i = b0; i <= b0 + e0; ++i)
+        for (int j = b1; j <= b1 + e1; ++j)
+            for (int k = b2; k <= b2 + e2; ++k) {
+                if ((unsigned)i < (unsigned)g.nbx && (unsigned)j < (unsigned)g.nby && (unsigned)k < (unsigned)g.nbz) {
+                    const int64_t blk = g.block_of(i, j, k);
+                    if (!alloc_done && alloc[blk] == 0) alloc[blk] = 1;
+                    touch_block(a, blk);
+                }
+            }
+}
+
 // One thread per particle, particles in base-node order. Reads x, F, m, V0;
 // writes x, v, C, F; scatters P2G(n+1) with one 16-byte reduction per node:
 // (momentum + force * dt, mass), the force folded in with the scene's dt. The
@@ -388,6 +427,9 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
     for (int q = 0; q < 9; ++q) Cm[q] = 0.0f;
     uint32_t heavy = 0u;
     const int gbase0 = base[0], gbase1 = base[1], gbase2 = base[2];
+    // no end weight exactly 0: the gather stencil spans all of base..base+2
+    const bool gather_full = wgt[0][0] != 0.0f && wgt[0][2] != 0.0f && wgt[1][0] != 0.0f && wgt[1][2] != 0.0f &&
+                             wgt[2][0] != 0.0f && wgt[2][2] != 0.0f;
     {
         const float4* __restrict__ cur_mv = S.cur_mv;
         const float cs = 4.0f * g.inv_dx * g.inv_dx;
@@ -455,6 +497,13 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
     const float ff = -4.0f * g.inv_dx * g.inv_dx * vol;
 #pragma unroll
     for (int q = 0; q < 9; ++q) sk[q] = sk[q] * ff;
+    // the contribution to a node at offset d is w (m v + (m C + dt S) d)
+    // (momentum plus force * dt), mass w m
+    float Mq[9], Pm[3];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Mq[q] = m * Cm[q] + dt * sk[q];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) Pm[a] = m * v[a];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         fx[a] = x[a] * g.inv_dx - 0.5f;
@@ -463,7 +512,8 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
 #pragma unroll
         for (int i = 0; i < 3; ++i) dd[a][i] = ((float)(base[a] + i) - fx[a] - 0.5f) * g.dx;
     }
-    if (base[0] != gbase0 || base[1] != gbase1 || base[2] != gbase2) heavy = 0u;
+    const bool same_base = base[0] == gbase0 && base[1] == gbase1 && base[2] == gbase2;
+    if (!same_base) heavy = 0u;
     {
         const int r0 = base[0] - g.ox, r1 = base[1] - g.oy, r2 = base[2] - g.oz;
         const bool inside = (unsigned)r0 <= (unsigned)(g.ex() - 3) && (unsigned)r1 <= (unsigned)(g.ey() - 3) &&
@@ -475,35 +525,29 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
             float4* df = next.f + g.node_rel(r0, r1, r2);
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                // momentum direction v + C d and stress S d, summed axis by axis
-                float qi[3], si[3];
+                // m v + (m C + dt S) d, summed axis by axis
+                float ui[3];
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    qi[a] = v[a] + Cm[3 * a] * dd[0][i];
-                    si[a] = sk[3 * a] * dd[0][i];
-                }
+                for (int a = 0; a < 3; ++a) ui[a] = Pm[a] + Mq[3 * a] * dd[0][i];
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    float qj[3], sj[3];
+                    float uj[3];
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        qj[a] = qi[a] + Cm[3 * a + 1] * dd[1][j];
-                        sj[a] = si[a] + sk[3 * a + 1] * dd[1][j];
-                    }
+                    for (int a = 0; a < 3; ++a) uj[a] = ui[a] + Mq[3 * a + 1] * dd[1][j];
                     const float wij = wgt[0][i] * wgt[1][j];
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const float w = wij * wgt[2][k];
                         const float mc = w * m;
-                        const float wdt = w * dt;
                         const int64_t off = i * EYZ + j * EZ + k;
-                        const float s0 = sj[0] + sk[2] * dd[2][k], s1 = sj[1] + sk[5] * dd[2][k],
-                                    s2 = sj[2] + sk[8] * dd[2][k];
-                        red_v4(dmv + off, (qj[0] + Cm[2] * dd[2][k]) * mc + s0 * wdt,
-                               (qj[1] + Cm[5] * dd[2][k]) * mc + s1 * wdt, (qj[2] + Cm[8] * dd[2][k]) * mc + s2 * wdt,
-                               mc);
-                        if (mc <= 1e-6f && !(heavy & (1u << (9 * i + 3 * j + k))))
-                            red_v4(df + off, s0 * w, s1 * w, s2 * w, 0.0f);
+                        red_v4(dmv + off, (uj[0] + Mq[2] * dd[2][k]) * w, (uj[1] + Mq[5] * dd[2][k]) * w,
+                               (uj[2] + Mq[8] * dd[2][k]) * w, mc);
+                        if (mc <= 1e-6f && !(heavy & (1u << (9 * i + 3 * j + k)))) {
+                            const float d0 = dd[0][i], d1 = dd[1][j], d2 = dd[2][k];
+                            red_v4(df + off, ((sk[0] * d0 + sk[1] * d1) + sk[2] * d2) * w,
+                                   ((sk[3] * d0 + sk[4] * d1) + sk[5] * d2) * w,
+                                   ((sk[6] * d0 + sk[7] * d1) + sk[8] * d2) * w, 0.0f);
+                        }
                     }
                 }
             }
@@ -517,18 +561,17 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
                 if (id < 0) { ++dropped; continue; }
                 const float d0 = pick3(dd[0], i), d1 = pick3(dd[1], j), d2 = pick3(dd[2], k);
                 const float mc = w * m;
-                const float s0 = (sk[0] * d0 + sk[1] * d1) + sk[2] * d2;
-                const float s1 = (sk[3] * d0 + sk[4] * d1) + sk[5] * d2;
-                const float s2 = (sk[6] * d0 + sk[7] * d1) + sk[8] * d2;
-                const float wdt = w * dt;
-                red_v4(next.mv + id, (v[0] + ((Cm[0] * d0 + Cm[1] * d1) + Cm[2] * d2)) * mc + s0 * wdt,
-                       (v[1] + ((Cm[3] * d0 + Cm[4] * d1) + Cm[5] * d2)) * mc + s1 * wdt,
-                       (v[2] + ((Cm[6] * d0 + Cm[7] * d1) + Cm[8] * d2)) * mc + s2 * wdt, mc);
-                if (mc <= 1e-6f) red_v4(next.f + id, s0 * w, s1 * w, s2 * w, 0.0f);
+                red_v4(next.mv + id, (Pm[0] + ((Mq[0] * d0 + Mq[1] * d1) + Mq[2] * d2)) * w,
+                       (Pm[1] + ((Mq[3] * d0 + Mq[4] * d1) + Mq[5] * d2)) * w,
+                       (Pm[2] + ((Mq[6] * d0 + Mq[7] * d1) + Mq[8] * d2)) * w, mc);
+                if (mc <= 1e-6f)
+                    red_v4(next.f + id, ((sk[0] * d0 + sk[1] * d1) + sk[2] * d2) * w,
+                           ((sk[3] * d0 + sk[4] * d1) + sk[5] * d2) * w, ((sk[6] * d0 + sk[7] * d1) + sk[8] * d2) * w,
+                           0.0f);
             }
         }
     }
-    mark_stencil_blocks(g, S.next, S.alloc, base, wgt[0], wgt[1], wgt[2]);
+    mark_stencil_blocks_warp(g, S.next, S.alloc, base, wgt[0], wgt[1], wgt[2], same_base && gather_full);
     if (!fin) atomicOr(S.status, ERR_NONFINITE);
     if (dropped) {
         atomicOr(S.status, ERR_ESCAPE);
