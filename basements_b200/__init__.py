@@ -162,6 +162,10 @@ _SIGS = {
     "bm_batch_sync": (_st, [_h, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "bm_batch_light_node_suspects": (_st, [_h, C.POINTER(C.c_int64)]),
     "bm_batch_set_graph": (_st, [_h, C.c_int32]),
+    "bm_batch_profile_enable": (_st, [_h, C.c_int32]),
+    "bm_batch_profile_read": (_st, [_h, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "bm_batch_profile_reset": (_st, [_h]),
     "bm_batch_set_launch": (_st, [_h, C.c_int32, C.c_int32, C.c_int32]),
     "bm_batch_autotune": (_st, [_h, C.c_int32, C.POINTER(TuneResult)]),
     "bm_batch_timer_start": (_st, [_h]),
@@ -540,6 +544,22 @@ class Batch:
 
     def set_graph(self, on: bool):
         check(lib().bm_batch_set_graph(self._h, 1 if on else 0), "bm_batch_set_graph")
+
+    def profile(self, on=True):
+        """Per-phase CUDA-event timing (steps run eagerly while it is on)."""
+        check(lib().bm_batch_profile_enable(self._h, 1 if on else 0), "bm_batch_profile_enable")
+
+    def profile_reset(self):
+        check(lib().bm_batch_profile_reset(self._h), "bm_batch_profile_reset")
+
+    def profile_read(self):
+        cap = 32
+        names = (C.c_char_p * cap)()
+        ms = (C.c_double * cap)()
+        cnt = (C.c_int64 * cap)()
+        n = C.c_int32()
+        check(lib().bm_batch_profile_read(self._h, cap, names, ms, cnt, C.byref(n)), "bm_batch_profile_read")
+        return {names[i].decode(): (ms[i], cnt[i]) for i in range(n.value)}
 
     def set_launch(self, variant, sort_interval, bin_shift=0):
         check(lib().bm_batch_set_launch(self._h, int(variant), int(sort_interval), int(bin_shift)),

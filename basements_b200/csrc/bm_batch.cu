@@ -478,6 +478,42 @@ BM_API bm_status_t bm_batch_sync(bm_batch_t* b, int32_t* bad_scene, int64_t* esc
     return result;
 }
 
+BM_API bm_status_t bm_batch_profile_enable(bm_batch_t* b, int32_t on) {
+    if (!b) return invalid_arg("NULL handle");
+    b->w.profiling = on != 0;
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_batch_profile_read(bm_batch_t* b, int32_t cap, const char** names, double* total_ms,
+                                         int64_t* launches, int32_t* n_out) {
+    if (!b || !n_out) return invalid_arg("NULL argument");
+    DeviceGuard dg(b->w.device);
+    BM_CHECK_CUDA(cudaStreamSynchronize(b->w.stream));
+    b->w.fold_pending();
+    int32_t n = 0;
+    for (const auto& sl : b->w.slots) {
+        if (n >= cap) break;
+        if (names) names[n] = sl.name;
+        if (total_ms) total_ms[n] = sl.total_ms;
+        if (launches) launches[n] = sl.launches;
+        ++n;
+    }
+    *n_out = n;
+    return BM_OK;
+}
+
+BM_API bm_status_t bm_batch_profile_reset(bm_batch_t* b) {
+    if (!b) return invalid_arg("NULL handle");
+    DeviceGuard dg(b->w.device);
+    cudaStreamSynchronize(b->w.stream);
+    b->w.fold_pending();
+    for (auto& sl : b->w.slots) {
+        sl.total_ms = 0;
+        sl.launches = 0;
+    }
+    return BM_OK;
+}
+
 BM_API bm_status_t bm_batch_set_graph(bm_batch_t* b, int32_t on) {
     if (!b) return invalid_arg("NULL handle");
     b->use_graph = on != 0;

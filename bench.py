@@ -386,6 +386,13 @@ def run_batched(args):
     st, bad, esc = b.sync()
     if st != 0:
         raise RuntimeError(f"batched: scene {bad} reported status {st}")
+    # per-phase breakdown from a few eager steps after the timed region
+    b.profile(True)
+    b.profile_reset()
+    prof_steps = 4
+    b.step(prof_steps)
+    phases = {k: round(v[0] / prof_steps, 4) for k, v in b.profile_read().items() if v[1] > 0}
+    b.profile(False)
     b.close()
     value = n_tot * args.steps / (ms / 1e3)
     loop_steps = min(args.steps, 50)
@@ -394,6 +401,7 @@ def run_batched(args):
                         "(log-uniform, 8 ppc), friction angle 25-40 deg, E 1e5-1e6 Pa, dynamic M1 box",
             "scenes": len(scs), "particles": n_tot, "value": value, "unit": UNIT, "steps": args.steps,
             "ms_per_step": ms / args.steps, "timing": "CUDA events on the batch stream",
+            "phases_ms_per_step_eager": phases,
             "autotune": tune,
             "plain_loop": {"value": loop_rate, "unit": UNIT, "steps_per_scene": loop_steps,
                            "seconds": loop_secs,

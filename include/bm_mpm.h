@@ -293,6 +293,12 @@ BM_API bm_status_t bm_batch_sync(bm_batch_t* b, int32_t* bad_scene, int64_t* esc
 /* bm_solver_light_node_suspects summed over the batch's scenes. */
 BM_API bm_status_t bm_batch_light_node_suspects(bm_batch_t* b, int64_t* out);
 BM_API bm_status_t bm_batch_set_graph(bm_batch_t* b, int32_t on);
+/* Per-phase timing of the batch, as bm_solver_profile_*; while it is on the
+ * steps run eagerly (no graph replay), so each launch can be timed. */
+BM_API bm_status_t bm_batch_profile_enable(bm_batch_t* b, int32_t on);
+BM_API bm_status_t bm_batch_profile_read(bm_batch_t* b, int32_t cap, const char** names, double* total_ms,
+                                         int64_t* launches, int32_t* n_out);
+BM_API bm_status_t bm_batch_profile_reset(bm_batch_t* b);
 BM_API bm_status_t bm_batch_set_launch(bm_batch_t* b, int32_t variant, int32_t sort_interval, int32_t bin_shift);
 /* Times each candidate launch setting for `trial_steps` steps on this batch
  * (the state is saved before and restored after every trial, so tuning does
