@@ -27,6 +27,9 @@
 //   include/basements/core/math/matrix3.h:177-251,405-447  Matrix3 ops
 //   include/basements/physics/coupling/mpm_rigid_coupler.h:90-103  shape_inside
 //   include/basements/physics/coupling/mpm_rigid_coupler_pic.h:88-184  M1
+//   include/basements/physics/coupling/mpm_rigid_coupler.h:139-200  overlap
+//       fraction and tight world AABB of a shape
+//   research/mpm_rigid_coupling/couplers/m4_5_hybrid.h:104-257  M4.5a
 //   include/basements/physics/dynamics/integrator.h:19-57  rigid update
 //
 // Thresholds are the reference's float literals, converted to R, so both
@@ -474,6 +477,104 @@ template <class R> Reaction<R> m1_apply(Grid<R>& grid, const ColliderF& b, R dt)
                     ++out.nodes_inside;
                 }
     }
+    out.force = fsum;
+    out.torque = tsum;
+    return out;
+}
+
+// mpm_rigid_coupler.h:139-164: 1 at the centre, 0 at the surface; box
+// (1-|x|/hx)(1-|y|/hy)(1-|z|/hz), cylinder (1-|y|/L)(1-r/R), each clamped to [0,1].
+template <class R> R overlap_fraction(const ColliderF& b, const V3<R>& l) {
+    auto clamp01 = [](R v) { return v < R(0) ? R(0) : (v > R(1) ? R(1) : v); };
+    if (b.shape == 1) {
+        const R Rr = (R)b.half_extents[0], L = (R)b.half_extents[1];
+        const R r = std::sqrt(l.x * l.x + l.z * l.z);
+        const R axial = R(1) - std::abs(l.y) / std::max(L, R(1e-9f));
+        const R radial = R(1) - r / std::max(Rr, R(1e-9f));
+        return clamp01(axial) * clamp01(radial);
+    }
+    const R ux = clamp01(R(1) - std::abs(l.x) / std::max((R)b.half_extents[0], R(1e-9f)));
+    const R uy = clamp01(R(1) - std::abs(l.y) / std::max((R)b.half_extents[1], R(1e-9f)));
+    const R uz = clamp01(R(1) - std::abs(l.z) / std::max((R)b.half_extents[2], R(1e-9f)));
+    return ux * uy * uz;
+}
+
+// mpm_rigid_coupler.h:167-200: box |R| he per row; cylinder |a_i| L +
+// sqrt(max(0, 1 - a_i^2)) R with a the body's y axis in world coordinates.
+template <class R> V3<R> world_aabb_half(const ColliderF& b, const M3<R>& Rl2w) {
+    if (b.shape == 1) {
+        const R Rr = (R)b.half_extents[0], L = (R)b.half_extents[1];
+        auto perp = [](R a) { const R s = R(1) - a * a; return s > R(0) ? std::sqrt(s) : R(0); };
+        const R ax = Rl2w.m[0][1], ay = Rl2w.m[1][1], az = Rl2w.m[2][1];
+        return V3<R>(std::abs(ax) * L + perp(ax) * Rr, std::abs(ay) * L + perp(ay) * Rr,
+                     std::abs(az) * L + perp(az) * Rr);
+    }
+    const R hx = b.half_extents[0], hy = b.half_extents[1], hz = b.half_extents[2];
+    return V3<R>(std::abs(Rl2w.m[0][0]) * hx + std::abs(Rl2w.m[0][1]) * hy + std::abs(Rl2w.m[0][2]) * hz,
+                 std::abs(Rl2w.m[1][0]) * hx + std::abs(Rl2w.m[1][1]) * hy + std::abs(Rl2w.m[1][2]) * hz,
+                 std::abs(Rl2w.m[2][0]) * hx + std::abs(Rl2w.m[2][1]) * hy + std::abs(Rl2w.m[2][2]) * hz);
+}
+
+// m4_5_hybrid.h:104-212 with the M4_5a rule (:242-257): pass 1 sums the
+// overlap fraction of the nodes inside the shape over the allocated blocks
+// whose node-centre span meets the shape's tight AABB; pass 2 gives each such
+// node m_b = M frac / sum (skipped when m_b <= 0) and the mass-weighted
+// average of node and body velocity (an empty node, mass < 1e-9, takes the
+// body's). The reaction sums m_b (v_after - v_body) / dt and its moment.
+template <class R> Reaction<R> m45a_apply(Grid<R>& grid, const ColliderF& b, R dt) {
+    Reaction<R> out;
+    if (dt <= R(0)) return out;
+    const R dx = grid.dx;
+    const M3<R> Rl2w = M3<R>::from_quat(b.orientation[0], b.orientation[1], b.orientation[2], b.orientation[3]);
+    const M3<R> Rw2l = Rl2w.T();
+    const V3<R> ah = world_aabb_half<R>(b, Rl2w);
+    const V3<R> c(b.center[0], b.center[1], b.center[2]);
+    const V3<R> lo = c - ah, hi = c + ah;
+    auto visit = [&](auto&& fn) {
+        for (auto& kv : grid.blocks) {
+            Block<R>& blk = kv.second;
+            const V3<R> blo(((R)blk.ox + R(0.5f)) * dx, ((R)blk.oy + R(0.5f)) * dx, ((R)blk.oz + R(0.5f)) * dx);
+            const V3<R> bhi(((R)(blk.ox + 3) + R(0.5f)) * dx, ((R)(blk.oy + 3) + R(0.5f)) * dx,
+                            ((R)(blk.oz + 3) + R(0.5f)) * dx);
+            if (bhi.x < lo.x || blo.x > hi.x) continue;
+            if (bhi.y < lo.y || blo.y > hi.y) continue;
+            if (bhi.z < lo.z || blo.z > hi.z) continue;
+            for (int li = 0; li < 4; ++li)
+                for (int lj = 0; lj < 4; ++lj)
+                    for (int lk = 0; lk < 4; ++lk) {
+                        const V3<R> xn(((R)(blk.ox + li) + R(0.5f)) * dx, ((R)(blk.oy + lj) + R(0.5f)) * dx,
+                                       ((R)(blk.oz + lk) + R(0.5f)) * dx);
+                        const V3<R> local = Rw2l * (xn - c);
+                        if (!shape_inside<R>(b, local)) continue;
+                        fn(blk.n[li * 16 + lj * 4 + lk], xn, local);
+                    }
+        }
+    };
+    R frac_sum = 0;
+    visit([&](Node<R>&, const V3<R>&, const V3<R>& local) { frac_sum += overlap_fraction<R>(b, local); });
+    if (frac_sum < R(1e-9f)) return out;
+    const R per_frac = (R)b.mass / frac_sum;
+    const V3<R> vl(b.linear_velocity[0], b.linear_velocity[1], b.linear_velocity[2]);
+    const V3<R> w(b.angular_velocity[0], b.angular_velocity[1], b.angular_velocity[2]);
+    V3<R> fsum, tsum;
+    visit([&](Node<R>& n, const V3<R>& xn, const V3<R>& local) {
+        const R mb = per_frac * overlap_fraction<R>(b, local);
+        if (mb <= R(0)) return;
+        const V3<R> r = xn - c;
+        const V3<R> vb = vl + w.cross(r);
+        const bool was_active = n.active && n.m >= R(1e-9f);
+        const R old_m = was_active ? n.m : R(0);
+        const V3<R> old_v = was_active ? n.v : V3<R>(R(0));
+        V3<R> va = vb;
+        if (was_active) va = (old_v * old_m + vb * mb) / (old_m + mb);
+        n.active = true;
+        n.m = old_m + mb;
+        n.v = va;
+        const V3<R> dF = (va - vb) * (mb / dt);
+        fsum += dF;
+        tsum += r.cross(dF);
+        ++out.nodes_inside;
+    });
     out.force = fsum;
     out.torque = tsum;
     return out;

@@ -41,18 +41,18 @@ def box_drop_csv(ref_root: str):
     return cols, data, metrics
 
 
-def research_csv(ref_root: str, scene: str, summaries):
+def research_csv(ref_root: str, scene: str, summaries, method="M1"):
     """One scene's M1 time series and its summary rows, as the reference's
     research bench wrote them (research/mpm_rigid_coupling/bench_compare_all.cpp:
     tine_drag :215-292, foot_step :374-504, box_drop_dense :505-613,
     rover_wheel :614-800)."""
     base = os.path.join(ref_root, "research/mpm_rigid_coupling/outputs/csv")
-    with open(os.path.join(base, f"{scene}_M1.csv")) as f:
+    with open(os.path.join(base, f"{scene}_{method}.csv")) as f:
         rows = list(csv.reader(f))
     data = np.array([[float(v) for v in r] for r in rows[1:]], np.float64)
     names, values = [], []
     for summary in summaries:
-        with open(os.path.join(base, f"{scene}_M1_{summary}.csv")) as f:
+        with open(os.path.join(base, f"{scene}_{method}_{summary}.csv")) as f:
             m = list(csv.reader(f))
         names += m[0][1:]
         values += [float(v) for v in m[1][1:]]
@@ -116,7 +116,10 @@ def run_small_scene():
                 pos20=out["position"], vel20=out["velocity"], F20=out["F"], C20=out["C"])
 
 
-def m1_cases(n_cases=12, seed=7):
+def m1_cases(n_cases=12, seed=7, coupler="m1_apply"):
+    """Seeded grids (empty, tiny and normal node masses) and random box and
+    cylinder poses, each through one call of the reference's coupler
+    (MPMRigidCouplerPIC::apply, or M4_5a::apply for coupler="m45a_apply")."""
     rng = np.random.RandomState(seed)
     out = {k: [] for k in ("dx", "seed_ijk", "seed_vel", "seed_mass", "body", "dt", "force", "torque",
                            "nodes_inside", "grid_ijk", "grid_vel", "grid_mass", "grid_active")}
@@ -143,7 +146,7 @@ def m1_cases(n_cases=12, seed=7):
         dt = float(rng.choice([1e-4, 5e-5, 1.0 / 240, 0.0]))
         s = O.CpuSolver("ref", dx)
         s.grid_seed(ijk, vel, mass)
-        f, t, n = s.m1_apply(body, dt)
+        f, t, n = getattr(s, coupler)(body, dt)
         g = s.grid_nodes()
         out["dx"].append(dx)
         out["seed_ijk"].append(ijk)
@@ -235,6 +238,11 @@ def main():
     np.savez_compressed(os.path.join(HERE, "repose_pile.npz"), **repose_summary(a.ref_root))
     np.savez_compressed(os.path.join(HERE, "small_scene.npz"), **run_small_scene())
     np.savez_compressed(os.path.join(HERE, "m1_cases.npz"), **m1_cases())
+    np.savez_compressed(os.path.join(HERE, "m45a_cases.npz"), **m1_cases(16, 23, "m45a_apply"))
+    scenes_m45a = {}
+    for scene, summaries in (("box_drop", ("metrics",)),) + M1_SCENES:
+        scenes_m45a.update(research_csv(a.ref_root, scene, summaries, "M4.5a"))
+    np.savez_compressed(os.path.join(HERE, "m45a_scenes.npz"), **scenes_m45a)
     np.savez_compressed(os.path.join(HERE, "svd_cases.npz"), **svd_cases())
     np.savez_compressed(os.path.join(HERE, "constitutive.npz"), **constitutive())
     for f in sorted(os.listdir(HERE)):

@@ -1,5 +1,5 @@
-"""The reference's grid-only M1 research scenes, as a harness loop around any
-coupler that exposes ``apply``/``grid`` access (the CUDA solver or the oracle).
+"""The reference's grid-only research scenes, as a harness loop around a
+coupler (M1 or M4.5a) of the CUDA solver or of the oracle.
 
 The loop restates research/mpm_rigid_coupling/bench_compare_all.cpp in float32:
 
@@ -52,6 +52,11 @@ def _axis_angle_x(angle):
 
 
 SCENES = {
+    # scenario_box_drop.h (bench_compare_all.cpp:72-208)
+    "box_drop": dict(dx=0.1, seed_lo=(-3, 0, -3), seed_hi=(3, 2, 3), node_mass=0.01,
+                     domain=((-8, -4, -8), (16, 16, 16)), center=(0.0, 0.55, 0.0),
+                     half=(0.2, 0.2, 0.2), q=(1.0, 0.0, 0.0, 0.0), vel=(0, 0, 0), omg=(0, 0, 0),
+                     friction=0.5, mass=1.0, shape=0, steps=720, kinematic=False),
     # scenario_box_drop.h with box_mass = 9 (bench_compare_all.cpp:507)
     "box_drop_dense": dict(dx=0.1, seed_lo=(-3, 0, -3), seed_hi=(3, 2, 3), node_mass=0.01,
                            domain=((-8, -4, -8), (16, 16, 16)), center=(0.0, 0.55, 0.0),
@@ -86,16 +91,21 @@ def tine_start(dx=0.05):
 
 
 class GpuGrid:
-    """The CUDA solver's grid (bm.MPMSolver) behind the loop."""
+    """The CUDA solver's grid (bm.MPMSolver) behind the loop; coupler "m1" or
+    "m45a"."""
 
-    def __init__(self, bm, sc):
+    def __init__(self, bm, sc, coupler="m1"):
         self.bm = bm
+        self.coupler = coupler
         self.s = bm.MPMSolver(sc["dx"], domain=sc["domain"])
         ijk = _seed_block(sc["seed_lo"], sc["seed_hi"])
         self.s.seed_grid(ijk, np.zeros((len(ijk), 3), np.float32), np.full(len(ijk), sc["node_mass"], np.float32))
 
     def apply(self, body, dt):
-        return self.s.m1_apply(self.bm.make_collider(**body), float(dt))
+        c = self.bm.make_collider(**body)
+        if self.coupler == "m45a":
+            return self.s.m45a_apply(c, float(dt))
+        return self.s.m1_apply(c, float(dt))
 
     def gravity_floor(self, g, dt):
         grid = self.s.get_grid()
@@ -111,14 +121,18 @@ class GpuGrid:
 class OracleGrid:
     """The oracle's grid (oracle.CpuSolver, reference build or port) behind the loop."""
 
-    def __init__(self, O, kind, sc):
+    def __init__(self, O, kind, sc, coupler="m1"):
         self.O = O
+        self.coupler = coupler
         self.s = O.CpuSolver(kind, sc["dx"])
         ijk = _seed_block(sc["seed_lo"], sc["seed_hi"])
         self.s.grid_seed(ijk, np.zeros((len(ijk), 3), np.float32), np.full(len(ijk), sc["node_mass"], np.float32))
 
     def apply(self, body, dt):
-        return self.s.m1_apply(self.O.collider(**body), float(dt))
+        c = self.O.collider(**body)
+        if self.coupler == "m45a":
+            return self.s.m45a_apply(c, float(dt))
+        return self.s.m1_apply(c, float(dt))
 
     def gravity_floor(self, g, dt):
         n = self.s.grid_nodes()

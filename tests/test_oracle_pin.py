@@ -69,8 +69,11 @@ def test_small_scene_bit_exact_vs_reference_fixture():
         assert np.array_equal(bits(p[a]), bits(d[b])), a
 
 
-def test_m1_bit_exact_vs_reference_fixture():
-    d = load("m1_cases.npz")
+@pytest.mark.parametrize("coupler", ["m1", "m45a"])
+def test_coupler_bit_exact_vs_reference_fixture(coupler):
+    """One call of the coupler on seeded grids, against the reference's
+    MPMRigidCouplerPIC::apply (m1_cases.npz) or M4_5a::apply (m45a_cases.npz)."""
+    d = load(f"{coupler}_cases.npz")
     off = {k: np.concatenate([[0], np.cumsum(d[k + "_len"])]) for k in ("seed_ijk", "grid_ijk")}
     for c in range(len(d["dx"])):
         sl = slice(off["seed_ijk"][c], off["seed_ijk"][c + 1])
@@ -78,7 +81,7 @@ def test_m1_bit_exact_vs_reference_fixture():
         s.grid_seed(d["seed_ijk"][sl], d["seed_vel"][sl], d["seed_mass"][sl])
         b = d["body"][c]
         body = O.collider(b[0:3], b[7:10], b[3:7], b[10:13], b[13:16], b[16], b[17], int(b[18]))
-        f, t, n = s.m1_apply(body, float(d["dt"][c]))
+        f, t, n = getattr(s, f"{coupler}_apply")(body, float(d["dt"][c]))
         assert n == d["nodes_inside"][c]
         assert np.array_equal(bits(f), bits(d["force"][c])) and np.array_equal(bits(t), bits(d["torque"][c]))
         g = s.grid_nodes()
@@ -133,6 +136,30 @@ def test_m1_research_scenes_reproduce_reference_csv(scene):
     if scene == "foot_step":
         down, up = L.rebound(rows)
         assert abs(down - vals["v_down_peak"]) <= 2e-6 * abs(vals["v_down_peak"]) and up == vals["v_up_peak"]
+
+
+@pytest.mark.parametrize("scene", ["box_drop", "box_drop_dense", "foot_step", "tine_drag", "rover_wheel"])
+def test_m45a_research_scenes_reproduce_reference_csv(scene):
+    """The grid-only research scenes with the M4.5a sweep coupler
+    (m4_5_hybrid.h:242-257), run by the float32 harness loop around the float
+    restatement, against the reference's shipped *_M4.5a CSVs."""
+    from tests import m1_scene_loop as L
+    d = load("m45a_scenes.npz")
+    ref = d[scene + "_rows"]
+    vals = dict(zip(d[scene + "_metric_names"], d[scene + "_metric_values"]))
+    rows = L.run(scene, L.OracleGrid(O, "f32", L.SCENES[scene], "m45a"))
+    if scene == "tine_drag":
+        fx, fy, n = L.tine_summary(rows)
+        rows = rows[::4]
+        assert rows.shape == ref.shape
+        np.testing.assert_allclose(rows[:, 1:], ref[:, 1:], rtol=2e-6, atol=1e-5)
+        assert n == vals["samples"]
+        assert abs(fx - vals["avg_draft_fx_n"]) <= 2e-6 * abs(vals["avg_draft_fx_n"])
+        return
+    assert rows.shape == ref.shape
+    np.testing.assert_allclose(rows[:, 1:8], ref[:, 1:8], rtol=2e-6, atol=1e-6)
+    assert np.array_equal(rows[:, 9], ref[:, 9])
+    assert abs(np.abs(rows[:, 7]).max() - vals["max_abs_total_p_y"]) <= 2e-6 * vals["max_abs_total_p_y"]
 
 
 def test_rigid_drift_pic_reproduces_reference_csv():
