@@ -30,6 +30,8 @@
 //   include/basements/physics/coupling/mpm_rigid_coupler.h:139-200  overlap
 //       fraction and tight world AABB of a shape
 //   research/mpm_rigid_coupling/couplers/m4_5_hybrid.h:104-257  M4.5a
+//   include/basements/physics/coupling/mpm_rigid_coupler.h:106-132  outward normal
+//   src/physics/coupling/mpm_rigid_coupler.cpp:58-143  M0 (Dirichlet)
 //   include/basements/physics/dynamics/integrator.h:19-57  rigid update
 //
 // Thresholds are the reference's float literals, converted to R, so both
@@ -575,6 +577,92 @@ template <class R> Reaction<R> m45a_apply(Grid<R>& grid, const ColliderF& b, R d
         tsum += r.cross(dF);
         ++out.nodes_inside;
     });
+    out.force = fsum;
+    out.torque = tsum;
+    return out;
+}
+
+// mpm_rigid_coupler.h:106-132: outward normal of the closest face in the
+// body frame. Cylinder: the cap (0, +-1, 0) when the axial distance is the
+// smaller, else radial (x/r, 0, z/r), or (1, 0, 0) on the axis. Box: the
+// axis of the smallest face distance, x before y before z on ties.
+template <class R> V3<R> outward_normal_local(const ColliderF& b, const V3<R>& l) {
+    if (b.shape == 1) {
+        const R Rr = (R)b.half_extents[0], L = (R)b.half_extents[1];
+        const R r = std::sqrt(l.x * l.x + l.z * l.z);
+        const R axial = L - std::abs(l.y);
+        const R radial = Rr - r;
+        if (axial < radial) return V3<R>(R(0), l.y >= R(0) ? R(1) : R(-1), R(0));
+        if (r > R(1e-9f)) return V3<R>(l.x / r, R(0), l.z / r);
+        return V3<R>(R(1), R(0), R(0));
+    }
+    const R dx = (R)b.half_extents[0] - std::abs(l.x);
+    const R dy = (R)b.half_extents[1] - std::abs(l.y);
+    const R dz = (R)b.half_extents[2] - std::abs(l.z);
+    if (dx <= dy && dx <= dz) return V3<R>(l.x >= R(0) ? R(1) : R(-1), R(0), R(0));
+    if (dy <= dz) return V3<R>(R(0), l.y >= R(0) ? R(1) : R(-1), R(0));
+    return V3<R>(R(0), R(0), l.z >= R(0) ? R(1) : R(-1));
+}
+
+// mpm_rigid_coupler.cpp:58-143 (M0, Dirichlet): over the allocated blocks
+// meeting the box-formula AABB, every node with mass > 1e-8 inside the shape
+// keeps its normal velocity no slower outward than the body's (n = the
+// closest face's normal in world, normalised) and blends its tangential
+// velocity toward the body's by min(1, friction); its mass is unchanged. The
+// reaction is minus the momentum change over dt, and its moment.
+template <class R> Reaction<R> m0_apply(Grid<R>& grid, const ColliderF& b, R dt) {
+    Reaction<R> out;
+    if (dt <= R(0)) return out;
+    const R dx = grid.dx;
+    const M3<R> Rl2w = M3<R>::from_quat(b.orientation[0], b.orientation[1], b.orientation[2], b.orientation[3]);
+    const M3<R> Rw2l = Rl2w.T();
+    const R hx = b.half_extents[0], hy = b.half_extents[1], hz = b.half_extents[2];
+    const V3<R> ah(std::abs(Rl2w.m[0][0]) * hx + std::abs(Rl2w.m[0][1]) * hy + std::abs(Rl2w.m[0][2]) * hz,
+                   std::abs(Rl2w.m[1][0]) * hx + std::abs(Rl2w.m[1][1]) * hy + std::abs(Rl2w.m[1][2]) * hz,
+                   std::abs(Rl2w.m[2][0]) * hx + std::abs(Rl2w.m[2][1]) * hy + std::abs(Rl2w.m[2][2]) * hz);
+    const V3<R> c(b.center[0], b.center[1], b.center[2]);
+    const V3<R> lo = c - ah, hi = c + ah;
+    const V3<R> vl(b.linear_velocity[0], b.linear_velocity[1], b.linear_velocity[2]);
+    const V3<R> w(b.angular_velocity[0], b.angular_velocity[1], b.angular_velocity[2]);
+    const R fr = std::min(R(1), (R)b.friction);
+    V3<R> fsum, tsum;
+    for (auto& kv : grid.blocks) {
+        Block<R>& blk = kv.second;
+        const V3<R> blo(((R)blk.ox + R(0.5f)) * dx, ((R)blk.oy + R(0.5f)) * dx, ((R)blk.oz + R(0.5f)) * dx);
+        const V3<R> bhi(((R)(blk.ox + 3) + R(0.5f)) * dx, ((R)(blk.oy + 3) + R(0.5f)) * dx,
+                        ((R)(blk.oz + 3) + R(0.5f)) * dx);
+        if (bhi.x < lo.x || blo.x > hi.x) continue;
+        if (bhi.y < lo.y || blo.y > hi.y) continue;
+        if (bhi.z < lo.z || blo.z > hi.z) continue;
+        for (int li = 0; li < 4; ++li)
+            for (int lj = 0; lj < 4; ++lj)
+                for (int lk = 0; lk < 4; ++lk) {
+                    Node<R>& n = blk.n[li * 16 + lj * 4 + lk];
+                    if (!n.active || n.m <= R(1e-8f)) continue;
+                    const V3<R> xn(((R)(blk.ox + li) + R(0.5f)) * dx, ((R)(blk.oy + lj) + R(0.5f)) * dx,
+                                   ((R)(blk.oz + lk) + R(0.5f)) * dx);
+                    const V3<R> local = Rw2l * (xn - c);
+                    if (!shape_inside<R>(b, local)) continue;
+                    const V3<R> r = xn - c;
+                    const V3<R> vb = vl + w.cross(r);
+                    const V3<R> vn_ = n.v;
+                    const V3<R> nw0 = Rl2w * outward_normal_local<R>(b, local);
+                    const R len = nw0.length();
+                    const V3<R> nw = len < R(1e-6f) ? V3<R>(R(0)) : nw0 / len;
+                    const R vn_node = vn_.dot(nw);
+                    const R vn_body = vb.dot(nw);
+                    const R vn_clamped = std::max(vn_node, vn_body);
+                    const V3<R> vt_node = vn_ - nw * vn_node;
+                    const V3<R> vt_body = vb - nw * vn_body;
+                    const V3<R> vt_new = vt_node + (vt_body - vt_node) * fr;
+                    const V3<R> va = nw * vn_clamped + vt_new;
+                    const V3<R> dp = (va - vn_) * n.m;
+                    n.v = va;
+                    fsum = fsum - dp / dt;
+                    tsum = tsum - r.cross(dp) / dt;
+                    ++out.nodes_inside;
+                }
+    }
     out.force = fsum;
     out.torque = tsum;
     return out;

@@ -92,6 +92,7 @@ def load(kind: str):
         "g2p": fn("g2p", None, C.c_void_p, C.c_float),
         "m1_apply": fn("m1_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
         "m45a_apply": fn("m45a_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
+        "m0_apply": fn("m0_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
         "grid_num_nodes": fn("grid_num_nodes", C.c_int64, C.c_void_p),
         "grid_get": fn("grid_get", C.c_int64, C.c_void_p, _i32, _f, _f, _f, _u8, C.c_int64),
         "grid_seed": fn("grid_seed", None, C.c_void_p, C.c_int64, _i32, _f, _f),
@@ -220,6 +221,12 @@ class CpuSolver:
     def m1_apply(self, body: OrcCollider, dt):
         r = np.zeros(6, np.float32)
         n = self.api["m1_apply"](self.h, C.byref(body), dt, _p(r))
+        return r[:3].copy(), r[3:].copy(), int(n)
+
+    def m0_apply(self, body: OrcCollider, dt):
+        """The M0 Dirichlet coupler (mpm_rigid_coupler.cpp:58-143)."""
+        r = np.zeros(6, np.float32)
+        n = self.api["m0_apply"](self.h, C.byref(body), dt, _p(r))
         return r[:3].copy(), r[3:].copy(), int(n)
 
     def m45a_apply(self, body: OrcCollider, dt):

@@ -59,6 +59,8 @@ ORC_EXPORT void ORC(grid_update)(void* h, float dt);
 ORC_EXPORT void ORC(g2p)(void* h, float dt);
 /* reaction: force[3], torque[3]; returns nodes_inside */
 ORC_EXPORT int ORC(m1_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
+/* the M0 Dirichlet coupler (MPMRigidCoupler); same reaction layout */
+ORC_EXPORT int ORC(m0_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
 /* the M4.5a two-pass sweep coupler; same reaction layout */
 ORC_EXPORT int ORC(m45a_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
 ORC_EXPORT int64_t ORC(grid_num_nodes)(void* h);

@@ -133,6 +133,13 @@ ORC_EXPORT int orc_m1_apply(void* h, const orc_collider_t* body, float dt, float
     return r.nodes_inside;
 }
 
+ORC_EXPORT int orc_m0_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
+    Reaction<R> r = m0_apply<R>(sv(h)->grid, to_collider(body), (R)dt);
+    reaction6[0] = (float)r.force.x; reaction6[1] = (float)r.force.y; reaction6[2] = (float)r.force.z;
+    reaction6[3] = (float)r.torque.x; reaction6[4] = (float)r.torque.y; reaction6[5] = (float)r.torque.z;
+    return r.nodes_inside;
+}
+
 ORC_EXPORT int orc_m45a_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
     Reaction<R> r = m45a_apply<R>(sv(h)->grid, to_collider(body), (R)dt);
     reaction6[0] = (float)r.force.x; reaction6[1] = (float)r.force.y; reaction6[2] = (float)r.force.z;

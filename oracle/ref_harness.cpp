@@ -7,7 +7,9 @@
 // reference source is copied here: every computation below is a call into
 // the reference's MPMSolver (include/basements/physics/mpm/mpm_solver.h),
 // SVD (include/basements/core/math/svd.h), MPMRigidCouplerPIC
-// (include/basements/physics/coupling/mpm_rigid_coupler_pic.h), the M4.5a
+// (include/basements/physics/coupling/mpm_rigid_coupler_pic.h), the M0
+// Dirichlet coupler MPMRigidCoupler (src/physics/coupling/mpm_rigid_coupler.cpp,
+// compiled where it lies by oracle/Makefile), the M4.5a
 // sweep coupler (research/mpm_rigid_coupling/couplers/m4_5_hybrid.h) and
 // TimeIntegrator (include/basements/physics/dynamics/integrator.h).
 //
@@ -147,6 +149,13 @@ ORC_EXPORT void ref_g2p(void* h, float dt) {
 
 ORC_EXPORT int ref_m1_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
     cp::CouplingReaction r = cp::MPMRigidCouplerPIC::apply(sv(h)->get_grid_mutable(), to_state(body), dt);
+    reaction6[0] = r.force.x; reaction6[1] = r.force.y; reaction6[2] = r.force.z;
+    reaction6[3] = r.torque.x; reaction6[4] = r.torque.y; reaction6[5] = r.torque.z;
+    return r.nodes_inside;
+}
+
+ORC_EXPORT int ref_m0_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
+    cp::CouplingReaction r = cp::MPMRigidCoupler::apply(sv(h)->get_grid_mutable(), to_state(body), dt);
     reaction6[0] = r.force.x; reaction6[1] = r.force.y; reaction6[2] = r.force.z;
     reaction6[3] = r.torque.x; reaction6[4] = r.torque.y; reaction6[5] = r.torque.z;
     return r.nodes_inside;

@@ -60,6 +60,15 @@ def research_csv(ref_root: str, scene: str, summaries, method="M1"):
             f"{scene}_metric_names": np.array(names), f"{scene}_metric_values": np.array(values)}
 
 
+def drift_dirichlet_csv(ref_root: str):
+    """benchmarks/bench_mpm_rigid_drift.cpp (default --method dirichlet, M0):
+    the same unit box drop; its shipped time series."""
+    with open(os.path.join(ref_root, "outputs/figures/mpm_rigid_drift.csv")) as f:
+        rows = list(csv.reader(f))
+    return {"rigid_drift_columns": np.array(rows[0]),
+            "rigid_drift_rows": np.array([[float(v) for v in r] for r in rows[1:]], np.float64)}
+
+
 def drift_pic_csv(ref_root: str):
     """benchmarks/bench_mpm_rigid_drift.cpp --method pic (:24-178): a unit box
     dropped on a 5x3x5 grid patch through M1; its shipped time series."""
@@ -119,7 +128,8 @@ def run_small_scene():
 def m1_cases(n_cases=12, seed=7, coupler="m1_apply"):
     """Seeded grids (empty, tiny and normal node masses) and random box and
     cylinder poses, each through one call of the reference's coupler
-    (MPMRigidCouplerPIC::apply, or M4_5a::apply for coupler="m45a_apply")."""
+    (MPMRigidCouplerPIC::apply; M4_5a::apply for coupler="m45a_apply";
+    MPMRigidCoupler::apply, M0, for coupler="m0_apply")."""
     rng = np.random.RandomState(seed)
     out = {k: [] for k in ("dx", "seed_ijk", "seed_vel", "seed_mass", "body", "dt", "force", "torque",
                            "nodes_inside", "grid_ijk", "grid_vel", "grid_mass", "grid_active")}
@@ -243,6 +253,11 @@ def main():
     for scene, summaries in (("box_drop", ("metrics",)),) + M1_SCENES:
         scenes_m45a.update(research_csv(a.ref_root, scene, summaries, "M4.5a"))
     np.savez_compressed(os.path.join(HERE, "m45a_scenes.npz"), **scenes_m45a)
+    np.savez_compressed(os.path.join(HERE, "m0_cases.npz"), **m1_cases(16, 31, "m0_apply"))
+    scenes_m0 = drift_dirichlet_csv(a.ref_root)
+    for scene, summaries in (("box_drop", ("metrics",)),) + M1_SCENES:
+        scenes_m0.update(research_csv(a.ref_root, scene, summaries, "M0"))
+    np.savez_compressed(os.path.join(HERE, "m0_scenes.npz"), **scenes_m0)
     np.savez_compressed(os.path.join(HERE, "svd_cases.npz"), **svd_cases())
     np.savez_compressed(os.path.join(HERE, "constitutive.npz"), **constitutive())
     for f in sorted(os.listdir(HERE)):

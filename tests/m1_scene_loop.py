@@ -1,5 +1,5 @@
 """The reference's grid-only research scenes, as a harness loop around a
-coupler (M1 or M4.5a) of the CUDA solver or of the oracle.
+coupler (M0, M1 or M4.5a) of the CUDA solver or of the oracle.
 
 The loop restates research/mpm_rigid_coupling/bench_compare_all.cpp in float32:
 
@@ -91,8 +91,8 @@ def tine_start(dx=0.05):
 
 
 class GpuGrid:
-    """The CUDA solver's grid (bm.MPMSolver) behind the loop; coupler "m1" or
-    "m45a"."""
+    """The CUDA solver's grid (bm.MPMSolver) behind the loop; coupler "m0",
+    "m1" or "m45a"."""
 
     def __init__(self, bm, sc, coupler="m1"):
         self.bm = bm
@@ -102,10 +102,7 @@ class GpuGrid:
         self.s.seed_grid(ijk, np.zeros((len(ijk), 3), np.float32), np.full(len(ijk), sc["node_mass"], np.float32))
 
     def apply(self, body, dt):
-        c = self.bm.make_collider(**body)
-        if self.coupler == "m45a":
-            return self.s.m45a_apply(c, float(dt))
-        return self.s.m1_apply(c, float(dt))
+        return getattr(self.s, f"{self.coupler}_apply")(self.bm.make_collider(**body), float(dt))
 
     def gravity_floor(self, g, dt):
         grid = self.s.get_grid()
@@ -129,10 +126,7 @@ class OracleGrid:
         self.s.grid_seed(ijk, np.zeros((len(ijk), 3), np.float32), np.full(len(ijk), sc["node_mass"], np.float32))
 
     def apply(self, body, dt):
-        c = self.O.collider(**body)
-        if self.coupler == "m45a":
-            return self.s.m45a_apply(c, float(dt))
-        return self.s.m1_apply(c, float(dt))
+        return getattr(self.s, f"{self.coupler}_apply")(self.O.collider(**body), float(dt))
 
     def gravity_floor(self, g, dt):
         n = self.s.grid_nodes()

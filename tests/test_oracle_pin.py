@@ -69,10 +69,11 @@ def test_small_scene_bit_exact_vs_reference_fixture():
         assert np.array_equal(bits(p[a]), bits(d[b])), a
 
 
-@pytest.mark.parametrize("coupler", ["m1", "m45a"])
+@pytest.mark.parametrize("coupler", ["m0", "m1", "m45a"])
 def test_coupler_bit_exact_vs_reference_fixture(coupler):
     """One call of the coupler on seeded grids, against the reference's
-    MPMRigidCouplerPIC::apply (m1_cases.npz) or M4_5a::apply (m45a_cases.npz)."""
+    MPMRigidCoupler::apply (m0_cases.npz), MPMRigidCouplerPIC::apply
+    (m1_cases.npz) or M4_5a::apply (m45a_cases.npz)."""
     d = load(f"{coupler}_cases.npz")
     off = {k: np.concatenate([[0], np.cumsum(d[k + "_len"])]) for k in ("seed_ijk", "grid_ijk")}
     for c in range(len(d["dx"])):
@@ -138,16 +139,18 @@ def test_m1_research_scenes_reproduce_reference_csv(scene):
         assert abs(down - vals["v_down_peak"]) <= 2e-6 * abs(vals["v_down_peak"]) and up == vals["v_up_peak"]
 
 
+@pytest.mark.parametrize("coupler", ["m45a", "m0"])
 @pytest.mark.parametrize("scene", ["box_drop", "box_drop_dense", "foot_step", "tine_drag", "rover_wheel"])
-def test_m45a_research_scenes_reproduce_reference_csv(scene):
+def test_sweep_and_dirichlet_research_scenes_reproduce_reference_csv(scene, coupler):
     """The grid-only research scenes with the M4.5a sweep coupler
-    (m4_5_hybrid.h:242-257), run by the float32 harness loop around the float
-    restatement, against the reference's shipped *_M4.5a CSVs."""
+    (m4_5_hybrid.h:242-257) or the M0 Dirichlet coupler
+    (mpm_rigid_coupler.cpp:58-143), run by the float32 harness loop around
+    the float restatement, against the reference's shipped *_M4.5a / *_M0 CSVs."""
     from tests import m1_scene_loop as L
-    d = load("m45a_scenes.npz")
+    d = load(f"{coupler}_scenes.npz")
     ref = d[scene + "_rows"]
     vals = dict(zip(d[scene + "_metric_names"], d[scene + "_metric_values"]))
-    rows = L.run(scene, L.OracleGrid(O, "f32", L.SCENES[scene], "m45a"))
+    rows = L.run(scene, L.OracleGrid(O, "f32", L.SCENES[scene], coupler))
     if scene == "tine_drag":
         fx, fy, n = L.tine_summary(rows)
         rows = rows[::4]
@@ -160,6 +163,39 @@ def test_m45a_research_scenes_reproduce_reference_csv(scene):
     np.testing.assert_allclose(rows[:, 1:8], ref[:, 1:8], rtol=2e-6, atol=1e-6)
     assert np.array_equal(rows[:, 9], ref[:, 9])
     assert abs(np.abs(rows[:, 7]).max() - vals["max_abs_total_p_y"]) <= 2e-6 * vals["max_abs_total_p_y"]
+
+
+def test_rigid_drift_dirichlet_reproduces_reference_csv():
+    """outputs/figures/mpm_rigid_drift.csv, written by
+    benchmarks/bench_mpm_rigid_drift.cpp with its default method (M0). The
+    reference rebuilt here (oracle/_ref) and the float restatement agree with
+    each other exactly and with this file to 2.6e-7 relative: the file came
+    from a build that rounds M0's velocity blend differently."""
+    from tests import m1_scene_loop as L
+    ref = load("m0_scenes.npz")["rigid_drift_rows"]
+    rows = L.run("rigid_drift", L.OracleGrid(O, "f32", L.SCENES["rigid_drift"], "m0"))[:, L.DRIFT_COLUMNS]
+    assert rows.shape == ref.shape
+    np.testing.assert_allclose(rows[:, 1:7], ref[:, 1:7], rtol=1e-6, atol=1e-7)
+    assert np.array_equal(rows[:, 7], ref[:, 7])
+
+
+@pytest.mark.parametrize("kind", ["f32", "ref"])
+def test_dirichlet_unit_tests_restated(kind):
+    """tests/test_mpm_rigid_coupler.cpp:26-92 on the oracle (and the reference
+    build): a jet into the bottom face lifts the body and is clamped, a node
+    outside is untouched, friction 1 takes the body's tangential velocity,
+    an offset node gives a torque."""
+    if kind == "ref" and not O.available("ref"):
+        pytest.skip("reference harness oracle/_ref not built")
+    from tests import dirichlet_kats as K
+    for case in K.CASES:
+        s = O.CpuSolver(kind, 0.1)
+        s.grid_seed(np.array([case["node"]], np.int32), np.array([case["vel"]], np.float32),
+                    np.array([1.0], np.float32))
+        f, t, n = s.m0_apply(O.collider(**case["body"]), 1.0 / 60.0)
+        g = s.grid_nodes()
+        at = np.nonzero((g["ijk"] == np.array(case["node"])).all(axis=1))[0][0]
+        K.check(case, f, t, n, g["velocity"][at])
 
 
 def test_rigid_drift_pic_reproduces_reference_csv():
