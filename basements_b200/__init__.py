@@ -136,6 +136,9 @@ _SIGS = {
     "bm_solver_p2g": (_st, [_h, C.c_float]),
     "bm_solver_grid_update": (_st, [_h, C.c_float]),
     "bm_coupler_m1_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
+    "bm_coupler_m45a_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
+    "bm_coupler_m0_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
+    "bm_solver_set_coupler": (_st, [_h, C.c_int32]),
     "bm_solver_g2p": (_st, [_h, C.c_float]),
     "bm_solver_step_coupled": (_st, [_h, C.c_float, C.c_int32, C.POINTER(Collider), C.POINTER(Reaction)]),
     "bm_solver_get_reactions": (_st, [_h, C.c_int32, C.POINTER(Reaction)]),
@@ -366,6 +369,22 @@ class MPMSolver:
         r = Reaction()
         check(lib().bm_coupler_m1_apply(self._h, C.byref(body), dt, C.byref(r)), "bm_coupler_m1_apply")
         return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
+
+    def m45a_apply(self, body: Collider, dt):
+        """The M4.5a two-pass sweep coupler; same contract as m1_apply."""
+        r = Reaction()
+        check(lib().bm_coupler_m45a_apply(self._h, C.byref(body), dt, C.byref(r)), "bm_coupler_m45a_apply")
+        return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
+
+    def m0_apply(self, body: Collider, dt):
+        """The M0 Dirichlet coupler; same contract as m1_apply."""
+        r = Reaction()
+        check(lib().bm_coupler_m0_apply(self._h, C.byref(body), dt, C.byref(r)), "bm_coupler_m0_apply")
+        return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
+
+    def set_coupler(self, name: str):
+        """Coupler of step_coupled: "m1" (default), "m45a" or "m0"."""
+        check(lib().bm_solver_set_coupler(self._h, {"m1": 0, "m45a": 1, "m0": 2}[name]), "bm_solver_set_coupler")
 
     def step_coupled(self, dt, bodies, read_reactions=True):
         n = len(bodies)

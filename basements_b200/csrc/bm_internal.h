@@ -252,12 +252,25 @@ struct M1Params {
     float lo[3], hi[3];  // world AABB of the box formula
     float mb;            // per-node body mass
     float mb_over_dt;
+    float friction;      // the body's friction (M0)
     int shape;
     int scene;           // scene whose grid the body couples to
     int active;          // 0: dt <= 0 or AABB outside the box -> no work
     int bi0, bj0, bk0, nbi, nbj, nbk;  // candidate block range (relative to box)
 };
 bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* out);
+// M0 for one body over `candidates` blocks of the M1 frame (m1_prepare):
+// Dirichlet exchange on the nodes inside, reaction added into d_acc.
+void launch_m0(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt, double* d_acc,
+               cudaStream_t st);
+// M4.5a frame of one body of scene 0: the shape's tight AABB in lo/hi, the
+// body's mass in mb.
+bool m45a_prepare(const GridDesc& g, const bm_collider_t& b, float dt, M1Params* out);
+// The two passes of M4.5a for one body over `candidates` blocks (P.nbi *
+// P.nbj * P.nbk): Sigma frac into *d_frac_sum (zeroed by the caller), then the
+// exchange, reaction added into d_acc (7 doubles, zeroed by the caller).
+void launch_m45a(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt,
+                 double* d_frac_sum, double* d_acc, cudaStream_t st);
 // True when the candidate block ranges of two bodies of one scene intersect
 // (they may then write the same nodes).
 inline bool m1_blocks_overlap(const M1Params& a, const M1Params& b) {

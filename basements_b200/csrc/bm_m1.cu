@@ -26,37 +26,20 @@ namespace {
 
 using namespace rn;
 
-// mpm_rigid_coupler_pic.h:100-117 plus the candidate block range.
-__host__ __device__ bool m1_params(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* P) {
-    P->scene = scene;
-    P->active = 0;
-    P->nbi = P->nbj = P->nbk = 0;
-    P->bi0 = P->bj0 = P->bk0 = 0;
-    if (!(dt > 0.0f)) return false;
+// Matrix3::from_quaternion (matrix3.h:432-447), row-major.
+__host__ __device__ void body_rotation(const bm_collider_t& b, float R[9]) {
     const float w = b.orientation[0], x = b.orientation[1], y = b.orientation[2], z = b.orientation[3];
     const float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z), xy = mul(x, y), xz = mul(x, z), yz = mul(y, z);
     const float wx = mul(w, x), wy = mul(w, y), wz = mul(w, z);
-    float* R = P->R;
     R[0] = sub(1.0f, mul(2.0f, add(yy, zz))); R[1] = mul(2.0f, sub(xy, wz)); R[2] = mul(2.0f, add(xz, wy));
     R[3] = mul(2.0f, add(xy, wz)); R[4] = sub(1.0f, mul(2.0f, add(xx, zz))); R[5] = mul(2.0f, sub(yz, wx));
     R[6] = mul(2.0f, sub(xz, wy)); R[7] = mul(2.0f, add(yz, wx)); R[8] = sub(1.0f, mul(2.0f, add(xx, yy)));
-    const float hx = b.half_extents[0], hy = b.half_extents[1], hz = b.half_extents[2];
+}
+
+// Conservative candidate block range of P's AABB (lo, hi) in the box (the
+// exact float test runs per block); false when it misses the box.
+__host__ __device__ bool candidate_range(const GridDesc& g, M1Params* P) {
     const float dx = g.dx;
-    const float vol = mul(mul(mul(8.0f, hx), hy), hz);
-    const int approx = (int)roundf(dvd(vol, mul(mul(dx, dx), dx)));
-    P->mb = dvd(b.mass, (float)(approx > 1 ? approx : 1));
-    P->mb_over_dt = dvd(P->mb, dt);
-    for (int a = 0; a < 3; ++a) {
-        const float h = add(add(mul(fabsf(R[3 * a]), hx), mul(fabsf(R[3 * a + 1]), hy)), mul(fabsf(R[3 * a + 2]), hz));
-        P->lo[a] = sub(b.center[a], h);
-        P->hi[a] = add(b.center[a], h);
-        P->c[a] = b.center[a];
-        P->vl[a] = b.linear_velocity[a];
-        P->w[a] = b.angular_velocity[a];
-        P->he[a] = b.half_extents[a];
-    }
-    P->shape = b.shape;
-    // Conservative candidate block range (the exact float test runs per block).
     const int org[3] = {g.ox, g.oy, g.oz};
     const int nb[3] = {g.nbx, g.nby, g.nbz};
     int b0[3], n[3];
@@ -75,8 +58,290 @@ __host__ __device__ bool m1_params(const GridDesc& g, const bm_collider_t& b, fl
     }
     P->bi0 = b0[0]; P->bj0 = b0[1]; P->bk0 = b0[2];
     P->nbi = n[0]; P->nbj = n[1]; P->nbk = n[2];
+    return true;
+}
+
+// mpm_rigid_coupler_pic.h:100-117 plus the candidate block range.
+__host__ __device__ bool m1_params(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* P) {
+    P->scene = scene;
+    P->active = 0;
+    P->nbi = P->nbj = P->nbk = 0;
+    P->bi0 = P->bj0 = P->bk0 = 0;
+    if (!(dt > 0.0f)) return false;
+    float* R = P->R;
+    body_rotation(b, R);
+    const float hx = b.half_extents[0], hy = b.half_extents[1], hz = b.half_extents[2];
+    const float dx = g.dx;
+    const float vol = mul(mul(mul(8.0f, hx), hy), hz);
+    const int approx = (int)roundf(dvd(vol, mul(mul(dx, dx), dx)));
+    P->mb = dvd(b.mass, (float)(approx > 1 ? approx : 1));
+    P->mb_over_dt = dvd(P->mb, dt);
+    for (int a = 0; a < 3; ++a) {
+        const float h = add(add(mul(fabsf(R[3 * a]), hx), mul(fabsf(R[3 * a + 1]), hy)), mul(fabsf(R[3 * a + 2]), hz));
+        P->lo[a] = sub(b.center[a], h);
+        P->hi[a] = add(b.center[a], h);
+        P->c[a] = b.center[a];
+        P->vl[a] = b.linear_velocity[a];
+        P->w[a] = b.angular_velocity[a];
+        P->he[a] = b.half_extents[a];
+    }
+    P->shape = b.shape;
+    P->friction = b.friction;
+    if (!candidate_range(g, P)) return false;
     P->active = 1;
     return true;
+}
+
+// m4_5_hybrid.h:113-120: the M4.5a frame of one body. P->lo/hi is the
+// shape's tight AABB (shape_world_aabb_half, mpm_rigid_coupler.h:167-200) and
+// P->mb holds the body's mass (the per-node share is set by the sweep).
+bool m45a_params(const GridDesc& g, const bm_collider_t& b, float dt, M1Params* P) {
+    P->scene = 0;
+    P->active = 0;
+    P->nbi = P->nbj = P->nbk = 0;
+    P->bi0 = P->bj0 = P->bk0 = 0;
+    if (!(dt > 0.0f)) return false;
+    float* R = P->R;
+    body_rotation(b, R);
+    const float hx = b.half_extents[0], hy = b.half_extents[1], hz = b.half_extents[2];
+    for (int a = 0; a < 3; ++a) {
+        float h;
+        if (b.shape == 1) {
+            // |a_i| L + sqrt(max(0, 1 - a_i^2)) R, a = the body's y axis in world
+            const float ai = R[3 * a + 1];
+            const float s = sub(1.0f, mul(ai, ai));
+            const float perp = s > 0.0f ? std::sqrt(s) : 0.0f;
+            h = add(mul(fabsf(ai), hy), mul(perp, hx));
+        } else {
+            h = add(add(mul(fabsf(R[3 * a]), hx), mul(fabsf(R[3 * a + 1]), hy)), mul(fabsf(R[3 * a + 2]), hz));
+        }
+        P->lo[a] = sub(b.center[a], h);
+        P->hi[a] = add(b.center[a], h);
+        P->c[a] = b.center[a];
+        P->vl[a] = b.linear_velocity[a];
+        P->w[a] = b.angular_velocity[a];
+        P->he[a] = b.half_extents[a];
+    }
+    P->shape = b.shape;
+    P->friction = b.friction;
+    P->mb = b.mass;
+    P->mb_over_dt = 0.0f;
+    if (!candidate_range(g, P)) return false;
+    P->active = 1;
+    return true;
+}
+
+// Candidate block (cb) of body P in scene S: its (bi, bj, bk) and linear id.
+__device__ __forceinline__ void candidate_block(const M1Params& P, const GridDesc& g, int64_t cb, int& bi, int& bj,
+                                                int& bk) {
+    bk = P.bk0 + (int)(cb % P.nbk);
+    bj = P.bj0 + (int)((cb / P.nbk) % P.nbj);
+    bi = P.bi0 + (int)(cb / ((int64_t)P.nbk * P.nbj));
+}
+
+// Sum over the 64 threads (2 warps) of a CTA, added to *out when non-zero.
+template <int N>
+__device__ __forceinline__ void cta64_add(double (&vals)[N], double* out) {
+#pragma unroll
+    for (int q = 0; q < N; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
+    __shared__ double part[2][N];
+    const int tt = threadIdx.x;
+    if ((tt & 31) == 0) {
+#pragma unroll
+        for (int q = 0; q < N; ++q) part[tt >> 5][q] = vals[q];
+    }
+    __syncthreads();
+    if (tt < N) {
+        const double s = part[0][tt] + part[1][tt];
+        if (s != 0.0) atomicAdd(out + tt, s);
+    }
+}
+
+// shape_outward_normal_local (mpm_rigid_coupler.h:106-132): the outward
+// normal of the closest face in the body frame.
+__device__ __forceinline__ void outward_normal_local(const M1Params& P, const float l[3], float n[3]) {
+    n[0] = n[1] = n[2] = 0.0f;
+    if (P.shape == 1) {
+        const float r = __fsqrt_rn(add(mul(l[0], l[0]), mul(l[2], l[2])));
+        const float axial = sub(P.he[1], fabsf(l[1]));
+        const float radial = sub(P.he[0], r);
+        if (axial < radial) {
+            n[1] = l[1] >= 0.0f ? 1.0f : -1.0f;
+        } else if (r > 1e-9f) {
+            n[0] = dvd(l[0], r);
+            n[2] = dvd(l[2], r);
+        } else {
+            n[0] = 1.0f;
+        }
+        return;
+    }
+    const float d0 = sub(P.he[0], fabsf(l[0])), d1 = sub(P.he[1], fabsf(l[1])), d2 = sub(P.he[2], fabsf(l[2]));
+    if (d0 <= d1 && d0 <= d2) n[0] = l[0] >= 0.0f ? 1.0f : -1.0f;
+    else if (d1 <= d2) n[1] = l[1] >= 0.0f ? 1.0f : -1.0f;
+    else n[2] = l[2] >= 0.0f ? 1.0f : -1.0f;
+}
+
+__device__ __forceinline__ float dot3(const float a[3], const float b[3]) {
+    return add(add(mul(a[0], b[0]), mul(a[1], b[1])), mul(a[2], b[2]));
+}
+
+// M0, MPMRigidCoupler::apply (mpm_rigid_coupler.cpp:58-143): over the
+// visited blocks of the M1 frame, a node with mass > 1e-8 inside the shape
+// keeps its normal velocity no slower outward than the body's (n = the
+// closest face's normal in world, normalised) and blends its tangential
+// velocity toward the body's by min(1, friction); its mass is unchanged. The
+// reaction is -dp/dt and its moment, per CTA in double into acc.
+__global__ void __launch_bounds__(64) k_m0(SceneTable t, const M1Params* params, int cur, float dt, double* acc) {
+    const M1Params& P = params[0];
+    if (!P.active) return;
+    const int64_t cb = blockIdx.x;
+    if (cb >= (int64_t)P.nbi * P.nbj * P.nbk) return;
+    const SceneDev& S = t.scenes[P.scene];
+    const GridDesc g = S.g;
+    const GridAcc A = S.acc[cur];
+    int bi, bj, bk;
+    candidate_block(P, g, cb, bi, bj, bk);
+    const int64_t blin = g.block_of(bi, bj, bk);
+    const int tt = threadIdx.x;
+    double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (m1_block_visited(P, g, S.alloc, bi, bj, bk)) {
+        const int64_t id = g.node_of_block(blin, tt);
+        float4 nv = A.mv[id];
+        const float m = node_total_mass(nv, A.f[id]);
+        float r[3], l[3];
+        if (m > 1e-8f && coupler_node_local(P, g.dx, g.ox + 4 * bi + (tt >> 4), g.oy + 4 * bj + ((tt >> 2) & 3),
+                                            g.oz + 4 * bk + (tt & 3), r, l)) {
+            const float vb[3] = {add(P.vl[0], sub(mul(P.w[1], r[2]), mul(P.w[2], r[1]))),
+                                 add(P.vl[1], sub(mul(P.w[2], r[0]), mul(P.w[0], r[2]))),
+                                 add(P.vl[2], sub(mul(P.w[0], r[1]), mul(P.w[1], r[0])))};
+            float nl[3], nw[3];
+            outward_normal_local(P, l, nl);
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                nw[a] = add(add(mul(P.R[3 * a], nl[0]), mul(P.R[3 * a + 1], nl[1])), mul(P.R[3 * a + 2], nl[2]));
+            const float len = __fsqrt_rn(dot3(nw, nw));
+#pragma unroll
+            for (int a = 0; a < 3; ++a) nw[a] = len < 1e-6f ? 0.0f : dvd(nw[a], len);
+            const float v[3] = {nv.x, nv.y, nv.z};
+            const float vn_node = dot3(v, nw), vn_body = dot3(vb, nw);
+            const float vn_cl = vn_node < vn_body ? vn_body : vn_node;
+            const float fr = P.friction < 1.0f ? P.friction : 1.0f;
+            float va[3], dp[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float vt_node = sub(v[a], mul(nw[a], vn_node));
+                const float vt_body = sub(vb[a], mul(nw[a], vn_body));
+                const float vt_new = add(vt_node, mul(sub(vt_body, vt_node), fr));
+                va[a] = add(mul(nw[a], vn_cl), vt_new);
+                dp[a] = mul(sub(va[a], v[a]), m);
+            }
+            nv.x = va[0]; nv.y = va[1]; nv.z = va[2];
+            A.mv[id] = nv;
+            const bool tiny = fabsf(dt) < 1e-6f;  // Vec3 division guard of the reference
+            const float tq[3] = {sub(mul(r[1], dp[2]), mul(r[2], dp[1])), sub(mul(r[2], dp[0]), mul(r[0], dp[2])),
+                                 sub(mul(r[0], dp[1]), mul(r[1], dp[0]))};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                vals[a] = tiny ? 0.0f : -dvd(dp[a], dt);
+                vals[3 + a] = tiny ? 0.0f : -dvd(tq[a], dt);
+            }
+            vals[6] = 1;
+        }
+    }
+    cta64_add<7>(vals, acc);
+}
+
+// M4.5a pass 1 (m4_5_hybrid.h:126-146): the overlap fraction summed over the
+// nodes inside the shape, per CTA in double, into *frac_sum.
+__global__ void __launch_bounds__(64) k_m45a_sum(SceneTable t, const M1Params* params, int cur, double* frac_sum) {
+    const M1Params& P = params[0];
+    if (!P.active) return;
+    const int64_t cb = blockIdx.x;
+    if (cb >= (int64_t)P.nbi * P.nbj * P.nbk) return;
+    const SceneDev& S = t.scenes[P.scene];
+    const GridDesc g = S.g;
+    int bi, bj, bk;
+    candidate_block(P, g, cb, bi, bj, bk);
+    const int tt = threadIdx.x;
+    double vals[1] = {0.0};
+    if (m1_block_visited(P, g, S.alloc, bi, bj, bk)) {
+        float r[3], l[3];
+        if (coupler_node_local(P, g.dx, g.ox + 4 * bi + (tt >> 4), g.oy + 4 * bj + ((tt >> 2) & 3),
+                               g.oz + 4 * bk + (tt & 3), r, l))
+            vals[0] = coupler_overlap_fraction(P, l);
+    }
+    cta64_add<1>(vals, frac_sum);
+}
+
+// M4.5a pass 2 (m4_5_hybrid.h:148-208 with the M4_5a rule :242-257): each
+// inside node gets m_b = M frac / sum (skipped when m_b <= 0) and the
+// mass-weighted average of node and body velocity, as in M1; reaction into
+// acc (force, torque, count) per CTA in double. The sum arrives in double and
+// is used in float, the type of the reference's accumulator.
+__global__ void __launch_bounds__(64) k_m45a(SceneTable t, const M1Params* params, int cur, float dt,
+                                             const double* frac_sum, double* acc) {
+    const M1Params& P = params[0];
+    if (!P.active) return;
+    const int64_t cb = blockIdx.x;
+    if (cb >= (int64_t)P.nbi * P.nbj * P.nbk) return;
+    const float fs = (float)*frac_sum;
+    if (fs < 1e-9f) return;  // no overlap at all (m4_5_hybrid.h:147)
+    const float per_frac = dvd(P.mb, fs);
+    const SceneDev& S = t.scenes[P.scene];
+    const GridDesc g = S.g;
+    const GridAcc A = S.acc[cur];
+    int bi, bj, bk;
+    candidate_block(P, g, cb, bi, bj, bk);
+    const int64_t blin = g.block_of(bi, bj, bk);
+    const int tt = threadIdx.x;
+    double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (m1_block_visited(P, g, S.alloc, bi, bj, bk)) {
+        float r[3], l[3];
+        if (coupler_node_local(P, g.dx, g.ox + 4 * bi + (tt >> 4), g.oy + 4 * bj + ((tt >> 2) & 3),
+                               g.oz + 4 * bk + (tt & 3), r, l)) {
+            const float mb = mul(per_frac, coupler_overlap_fraction(P, l));
+            if (!(mb <= 0.0f)) {
+                const float vb[3] = {add(P.vl[0], sub(mul(P.w[1], r[2]), mul(P.w[2], r[1]))),
+                                     add(P.vl[1], sub(mul(P.w[2], r[0]), mul(P.w[0], r[2]))),
+                                     add(P.vl[2], sub(mul(P.w[0], r[1]), mul(P.w[1], r[0])))};
+                const int64_t id = g.node_of_block(blin, tt);
+                float4 nv = A.mv[id];
+                float4 nf = A.f[id];
+                const float m_tot = node_total_mass(nv, nf);
+                float va[3];
+                if (!(m_tot >= 1e-9f)) {  // inactive or below kInactiveNodeMassEpsilon: the body's velocity
+                    va[0] = vb[0]; va[1] = vb[1]; va[2] = vb[2];
+                    nv = make_float4(vb[0], vb[1], vb[2], 0.0f);
+                    nf.w = mb;
+                } else {
+                    const float mn = add(m_tot, mb);
+                    const float pa[3] = {add(mul(nv.x, m_tot), mul(vb[0], mb)), add(mul(nv.y, m_tot), mul(vb[1], mb)),
+                                         add(mul(nv.z, m_tot), mul(vb[2], mb))};
+                    if (fabsf(mn) < 1e-6f) {  // Vec3 division guard of the reference
+                        va[0] = va[1] = va[2] = 0.0f;
+                    } else {
+                        va[0] = dvd(pa[0], mn); va[1] = dvd(pa[1], mn); va[2] = dvd(pa[2], mn);
+                    }
+                    nv = make_float4(va[0], va[1], va[2], nv.w);
+                    nf.w = mn;
+                }
+                A.mv[id] = nv;
+                A.f[id] = nf;
+                touch_block(A, blin);
+                const float mbdt = dvd(mb, dt);
+                const float dF[3] = {mul(sub(va[0], vb[0]), mbdt), mul(sub(va[1], vb[1]), mbdt),
+                                     mul(sub(va[2], vb[2]), mbdt)};
+                vals[0] = dF[0]; vals[1] = dF[1]; vals[2] = dF[2];
+                vals[3] = sub(mul(r[1], dF[2]), mul(r[2], dF[1]));
+                vals[4] = sub(mul(r[2], dF[0]), mul(r[0], dF[2]));
+                vals[5] = sub(mul(r[0], dF[1]), mul(r[1], dF[0]));
+                vals[6] = 1;
+            }
+        }
+    }
+    cta64_add<7>(vals, acc);
 }
 
 // cand_prefix NULL: grid (max candidates, bodies), body = blockIdx.y.
@@ -281,6 +546,23 @@ inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 bool m1_prepare(const GridDesc& g, const bm_collider_t& b, float dt, int scene, M1Params* P) {
     return m1_params(g, b, dt, scene, P);
+}
+
+bool m45a_prepare(const GridDesc& g, const bm_collider_t& b, float dt, M1Params* P) {
+    return m45a_params(g, b, dt, P);
+}
+
+void launch_m0(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt, double* d_acc,
+               cudaStream_t st) {
+    if (candidates <= 0) return;
+    k_m0<<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, dt, d_acc);
+}
+
+void launch_m45a(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt,
+                 double* d_frac_sum, double* d_acc, cudaStream_t st) {
+    if (candidates <= 0) return;
+    k_m45a_sum<<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, d_frac_sum);
+    k_m45a<<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, dt, d_frac_sum, d_acc);
 }
 
 int64_t m1_max_candidates(const GridDesc& g, const float he[3]) {

@@ -96,4 +96,41 @@ __device__ __forceinline__ bool m1_node_inside(const M1Params& P, float dx, int 
     return inside;
 }
 
+// The node (i, j, k) in the body frame: r its centre relative to the body
+// centre, l = R^T r; true when it is inside the shape (the test of
+// m1_node_inside, for couplers that also need l).
+__device__ __forceinline__ bool coupler_node_local(const M1Params& P, float dx, int i, int j, int k, float r[3],
+                                                   float l[3]) {
+    using namespace rn;
+    const float xn[3] = {mul((float)i + 0.5f, dx), mul((float)j + 0.5f, dx), mul((float)k + 0.5f, dx)};
+    r[0] = sub(xn[0], P.c[0]);
+    r[1] = sub(xn[1], P.c[1]);
+    r[2] = sub(xn[2], P.c[2]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) l[a] = add(add(mul(P.R[a], r[0]), mul(P.R[3 + a], r[1])), mul(P.R[6 + a], r[2]));
+    if (P.shape == 1) {
+        const float r2 = add(mul(l[0], l[0]), mul(l[2], l[2]));
+        return fabsf(l[1]) <= P.he[1] && r2 <= mul(P.he[0], P.he[0]);
+    }
+    return fabsf(l[0]) <= P.he[0] && fabsf(l[1]) <= P.he[1] && fabsf(l[2]) <= P.he[2];
+}
+
+// shape_cell_overlap_fraction (mpm_rigid_coupler.h:139-164): 1 at the centre,
+// 0 at the surface; box (1-|x|/hx)(1-|y|/hy)(1-|z|/hz), cylinder
+// (1-|y|/L)(1-r/R), each factor clamped to [0, 1].
+__device__ __forceinline__ float coupler_overlap_fraction(const M1Params& P, const float l[3]) {
+    using namespace rn;
+    auto clamp01 = [](float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); };
+    if (P.shape == 1) {
+        const float r = __fsqrt_rn(add(mul(l[0], l[0]), mul(l[2], l[2])));
+        const float axial = sub(1.0f, dvd(fabsf(l[1]), fmaxf(P.he[1], 1e-9f)));
+        const float radial = sub(1.0f, dvd(r, fmaxf(P.he[0], 1e-9f)));
+        return mul(clamp01(axial), clamp01(radial));
+    }
+    const float ux = clamp01(sub(1.0f, dvd(fabsf(l[0]), fmaxf(P.he[0], 1e-9f))));
+    const float uy = clamp01(sub(1.0f, dvd(fabsf(l[1]), fmaxf(P.he[1], 1e-9f))));
+    const float uz = clamp01(sub(1.0f, dvd(fabsf(l[2]), fmaxf(P.he[2], 1e-9f))));
+    return mul(mul(ux, uy), uz);
+}
+
 }  // namespace bm

@@ -32,12 +32,15 @@ bm_status_t ensure_reactions(bm_solver* s, int n) {
     cudaFree(s->d_acc);
     cudaFree(s->d_react);
     cudaFree(s->d_params);
+    cudaFree(s->d_frac_sum);
     s->d_acc = nullptr;
     s->d_react = nullptr;
     s->d_params = nullptr;
+    s->d_frac_sum = nullptr;
     BM_CHECK_CUDA(cudaMalloc((void**)&s->d_acc, sizeof(double) * 7 * n));
     BM_CHECK_CUDA(cudaMalloc((void**)&s->d_react, sizeof(bm_reaction_t) * n));
     BM_CHECK_CUDA(cudaMalloc((void**)&s->d_params, sizeof(M1Params) * n));
+    BM_CHECK_CUDA(cudaMalloc((void**)&s->d_frac_sum, sizeof(double) * n));
     s->react_cap = n;
     return BM_OK;
 }
@@ -127,6 +130,55 @@ bm_status_t do_m1(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float
     return launch_status("m1");
 }
 
+bm_status_t do_m0(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt) {
+    bm_status_t st = ensure_reactions(s, std::max(1, n_bodies));
+    if (st != BM_OK) return st;
+    s->h_params.resize(n_bodies);
+    std::vector<M1Params>& hp = s->h_params;
+    for (int b = 0; b < n_bodies; ++b) m1_prepare(s->sc().dev.g, bodies[b], dt, 0, &hp[b]);
+    BM_CHECK_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(double) * 7 * n_bodies, s->w.stream));
+    if (n_bodies > 0)
+        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_params, hp.data(), sizeof(M1Params) * n_bodies, cudaMemcpyHostToDevice,
+                                      s->w.stream));
+    s->w.timed("m0_coupler", [&] {
+        for (int b = 0; b < n_bodies; ++b) {
+            const M1Params& P = hp[b];
+            if (!P.active) continue;
+            launch_m0(s->w.table(), s->d_params + b, (int64_t)P.nbi * P.nbj * P.nbk, s->w.cur, dt, s->d_acc + 7 * b,
+                      s->w.stream);
+        }
+    });
+    launch_reaction_finalize(s->d_acc, n_bodies, s->d_react, s->w.stream);
+    s->view = s->w.cur;
+    return launch_status("m0");
+}
+
+// The reference applies a coupler to one body at a time (ApplyFn,
+// bench_compare_all.cpp:50-51); each body's two passes run in order.
+bm_status_t do_m45a(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt) {
+    bm_status_t st = ensure_reactions(s, std::max(1, n_bodies));
+    if (st != BM_OK) return st;
+    s->h_params.resize(n_bodies);
+    std::vector<M1Params>& hp = s->h_params;
+    for (int b = 0; b < n_bodies; ++b) m45a_prepare(s->sc().dev.g, bodies[b], dt, &hp[b]);
+    BM_CHECK_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(double) * 7 * n_bodies, s->w.stream));
+    BM_CHECK_CUDA(cudaMemsetAsync(s->d_frac_sum, 0, sizeof(double) * n_bodies, s->w.stream));
+    if (n_bodies > 0)
+        BM_CHECK_CUDA(cudaMemcpyAsync(s->d_params, hp.data(), sizeof(M1Params) * n_bodies, cudaMemcpyHostToDevice,
+                                      s->w.stream));
+    s->w.timed("m45a_coupler", [&] {
+        for (int b = 0; b < n_bodies; ++b) {
+            const M1Params& P = hp[b];
+            if (!P.active) continue;
+            launch_m45a(s->w.table(), s->d_params + b, (int64_t)P.nbi * P.nbj * P.nbk, s->w.cur, dt,
+                        s->d_frac_sum + b, s->d_acc + 7 * b, s->w.stream);
+        }
+    });
+    launch_reaction_finalize(s->d_acc, n_bodies, s->d_react, s->w.stream);
+    s->view = s->w.cur;
+    return launch_status("m45a");
+}
+
 bm_status_t do_g2p(bm_solver* s, float dt) {
     if (!s->sc().grid_ready || !s->acc_valid) {
         set_last_error("g2p needs a grid from p2g / grid_update");
@@ -167,7 +219,10 @@ bm_status_t do_step(bm_solver* s, float dt, int32_t n_bodies, const bm_collider_
     if (st == BM_OK && s->acc_valid && s->folded[s->w.cur] && dt != s->fold_dt[s->w.cur]) s->acc_valid = false;
     if (st == BM_OK && !s->acc_valid) st = do_p2g(s);
     if (st == BM_OK) st = do_grid_update(s, dt);
-    if (st == BM_OK && n_bodies > 0) st = do_m1(s, n_bodies, bodies, dt);
+    if (st == BM_OK && n_bodies > 0)
+        st = s->coupler == BM_COUPLER_M45A ? do_m45a(s, n_bodies, bodies, dt)
+             : s->coupler == BM_COUPLER_M0 ? do_m0(s, n_bodies, bodies, dt)
+                                           : do_m1(s, n_bodies, bodies, dt);
     if (st == BM_OK) st = do_g2p2g(s, dt);
     return st;
 }
@@ -253,6 +308,7 @@ BM_API bm_status_t bm_solver_destroy(bm_solver_t* s) {
     cudaFree(s->d_acc);
     cudaFree(s->d_react);
     cudaFree(s->d_params);
+    cudaFree(s->d_frac_sum);
     delete s;
     return BM_OK;
 }
@@ -465,6 +521,43 @@ BM_API bm_status_t bm_coupler_m1_apply(bm_solver_t* s, const bm_collider_t* body
     if (st != BM_OK) return st;
     BM_CHECK_CUDA(cudaMemcpyAsync(out, s->d_react, sizeof(bm_reaction_t), cudaMemcpyDeviceToHost, s->w.stream));
     BM_CHECK_CUDA(cudaStreamSynchronize(s->w.stream));
+    return BM_OK;
+}
+
+namespace {
+// One coupler call of the split API: checks, the coupler, the reaction read back.
+bm_status_t coupler_call(bm_solver_t* s, const bm_collider_t* body, float dt, bm_reaction_t* out,
+                         bm_status_t (*coupler)(bm_solver*, int, const bm_collider_t*, float)) {
+    if (!s || !body || !out) return invalid_arg("NULL argument");
+    DeviceGuard dg(s->w.device);
+    std::memset(out, 0, sizeof(*out));
+    bm_status_t st = prepare(s);
+    if (st != BM_OK) return st;
+    if (!s->acc_valid && s->sc().n() > 0) {
+        set_last_error("the coupler needs a grid from p2g / grid_update");
+        return BM_ERR_STATE;
+    }
+    st = coupler(s, 1, body, dt);
+    if (st != BM_OK) return st;
+    BM_CHECK_CUDA(cudaMemcpyAsync(out, s->d_react, sizeof(bm_reaction_t), cudaMemcpyDeviceToHost, s->w.stream));
+    BM_CHECK_CUDA(cudaStreamSynchronize(s->w.stream));
+    return BM_OK;
+}
+}  // namespace
+
+BM_API bm_status_t bm_coupler_m0_apply(bm_solver_t* s, const bm_collider_t* body, float dt, bm_reaction_t* out) {
+    return coupler_call(s, body, dt, out, &do_m0);
+}
+
+BM_API bm_status_t bm_coupler_m45a_apply(bm_solver_t* s, const bm_collider_t* body, float dt, bm_reaction_t* out) {
+    return coupler_call(s, body, dt, out, &do_m45a);
+}
+
+BM_API bm_status_t bm_solver_set_coupler(bm_solver_t* s, int32_t coupler) {
+    if (!s) return invalid_arg("NULL handle");
+    if (coupler != BM_COUPLER_M1 && coupler != BM_COUPLER_M45A && coupler != BM_COUPLER_M0)
+        return invalid_arg("unknown coupler");
+    s->coupler = coupler;
     return BM_OK;
 }
 

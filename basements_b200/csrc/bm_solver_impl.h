@@ -23,7 +23,9 @@ struct bm_solver {
     double* d_acc = nullptr;
     bm_reaction_t* d_react = nullptr;
     bm::M1Params* d_params = nullptr;
+    double* d_frac_sum = nullptr;  // per body: the M4.5a overlap-fraction sum
     int react_cap = 0;
+    int32_t coupler = BM_COUPLER_M1;  // coupler of bm_solver_step_coupled
     std::vector<bm::M1Params> h_params;
 
     bm::SceneHost& sc() { return w.scenes[0]; }
@@ -56,6 +58,10 @@ bm_status_t do_p2g(bm_solver* s);
 bm_status_t do_grid_update(bm_solver* s, float dt);
 // M1 for each body in order on acc[cur]; reactions into s->d_react.
 bm_status_t do_m1(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt);
+// M0 for each body in order on acc[cur]; reactions into s->d_react.
+bm_status_t do_m0(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt);
+// M4.5a for each body in order on acc[cur]; reactions into s->d_react.
+bm_status_t do_m45a(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt);
 // The standalone G2P from acc[cur].
 bm_status_t do_g2p(bm_solver* s, float dt);
 // The particle order or grid contents changed behind the solver's back.

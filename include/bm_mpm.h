@@ -177,6 +177,36 @@ BM_API bm_status_t bm_coupler_m1_apply(bm_solver_t* s, const bm_collider_t* body
  * `out` (n_bodies entries) is written before the call returns. */
 BM_API bm_status_t bm_coupler_m1_apply_noalloc(bm_solver_t* s, int32_t n_bodies, const bm_collider_t* bodies,
                                                float dt, bm_reaction_t* out);
+/* The M4.5a two-pass sweep coupler (research/mpm_rigid_coupling/couplers/
+ * m4_5_hybrid.h:104-212, rule M4_5a :242-257): pass 1 sums the overlap
+ * fraction (mpm_rigid_coupler.h:139-164) of the nodes inside the shape over
+ * the allocated blocks meeting its tight AABB (:167-200); pass 2 gives each
+ * such node m_b = body mass * frac / sum and the mass-weighted average of node
+ * and body velocity. Same call contract as bm_coupler_m1_apply. The sum is
+ * taken in double on the device (the reference sums in float in hash-map
+ * order), so node states and the reaction agree with the reference to
+ * rounding rather than bit for bit. */
+BM_API bm_status_t bm_coupler_m45a_apply(bm_solver_t* s, const bm_collider_t* body, float dt,
+                                         bm_reaction_t* out);
+/* The M0 Dirichlet coupler, MPMRigidCoupler::apply
+ * (src/physics/coupling/mpm_rigid_coupler.cpp:58-143): over the allocated
+ * blocks meeting the box-formula AABB, each node of mass > 1e-8 inside the
+ * shape keeps its velocity along the closest face's outward normal
+ * (shape_outward_normal_local, mpm_rigid_coupler.h:106-132) at least the
+ * body's and blends its tangential velocity toward the body's by
+ * min(1, friction); node masses are unchanged. The reaction is -dp/dt and its
+ * moment. Same call contract as bm_coupler_m1_apply; the grid after the call
+ * matches the reference bit for bit, the reaction to its summation order. */
+BM_API bm_status_t bm_coupler_m0_apply(bm_solver_t* s, const bm_collider_t* body, float dt,
+                                       bm_reaction_t* out);
+/* Coupler that bm_solver_step_coupled applies to its bodies (each body in
+ * order, the ApplyFn table of bench_compare_all.cpp:50-70): BM_COUPLER_M1
+ * (default), BM_COUPLER_M45A or BM_COUPLER_M0. The batched and served forms
+ * and the tape use M1. */
+#define BM_COUPLER_M1 0
+#define BM_COUPLER_M45A 1
+#define BM_COUPLER_M0 2
+BM_API bm_status_t bm_solver_set_coupler(bm_solver_t* s, int32_t coupler);
 /* The G2P loop (:83-86). */
 BM_API bm_status_t bm_solver_g2p(bm_solver_t* s, float dt);
 /* P2G, grid update, M1 for each body in order, G2P, all on the handle's

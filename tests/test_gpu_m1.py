@@ -9,6 +9,9 @@
   foot_step, tine_drag, rover_wheel; 480-720 steps) and the rigid-drift
   benchmark's M1 run against their shipped CSVs;
 * the reference's cylinder inside-test KATs, probed through the coupler;
+* the M4.5a sweep and M0 Dirichlet couplers: the reference's per-call
+  fixtures, the research scenes' *_M4.5a / *_M0 CSVs, the M0 unit tests, the
+  Dirichlet rigid-drift output and a coupled particle scene;
 * a particle scene with a cylinder through bm_solver_step_coupled against the
   reference's split phases P2G -> update_grid -> apply -> G2P.
 """
@@ -59,6 +62,132 @@ def test_m1_matches_reference_fixtures():
         mask = np.ones(g["mass"].size, bool)
         mask[idx] = False
         assert np.all(g["mass"].reshape(-1)[mask] == 0)
+
+
+@pytest.mark.parametrize("coupler", ["m45a", "m0"])
+def test_sweep_and_dirichlet_match_reference_fixtures(coupler):
+    """One call of the CUDA M4.5a sweep or M0 Dirichlet coupler on the seeded
+    grids of m45a_cases.npz / m0_cases.npz (made by the reference's
+    M4_5a::apply / MPMRigidCoupler::apply). nodes_inside exactly; force and
+    torque to 1e-5 of their largest component (summed in double per CTA, in
+    float in hash-map order by the reference). M0's node update is per node,
+    so its grid is exact; M4.5a's overlap sum is taken in double on the
+    device, so its grid agrees to 1e-5 relative."""
+    d = np.load(os.path.join(GOLD, f"{coupler}_cases.npz"))
+    off = {k: np.concatenate([[0], np.cumsum(d[k + "_len"])]) for k in ("seed_ijk", "grid_ijk")}
+    for c in range(len(d["dx"])):
+        sl = slice(off["seed_ijk"][c], off["seed_ijk"][c + 1])
+        ijk = d["seed_ijk"][sl]
+        lo = ijk.min(0) - 8
+        hi = ijk.max(0) + 8
+        s = bm.MPMSolver(float(d["dx"][c]), domain=(tuple(lo), tuple(hi - lo)))
+        s.seed_grid(ijk, d["seed_vel"][sl], d["seed_mass"][sl])
+        body = bm.make_collider(**_body_from_row(d["body"][c]))
+        f, t, n = getattr(s, f"{coupler}_apply")(body, float(d["dt"][c]))
+        assert n == d["nodes_inside"][c], c
+        fr, tr = d["force"][c], d["torque"][c]
+        assert np.abs(f - fr).max() <= 1e-5 * max(np.abs(fr).max(), 1e-30) + 1e-30, (c, f, fr)
+        assert np.abs(t - tr).max() <= 1e-5 * max(np.abs(tr).max(), 1e-30) + 1e-30, (c, t, tr)
+        g = s.get_grid()
+        gs = slice(off["grid_ijk"][c], off["grid_ijk"][c + 1])
+        idx = dense_index(g, d["grid_ijk"][gs])
+        if coupler == "m0":
+            assert np.array_equal(g["velocity"].reshape(-1, 3)[idx], d["grid_vel"][gs]), c
+            assert np.array_equal(g["mass"].reshape(-1)[idx], d["grid_mass"][gs]), c
+        else:
+            np.testing.assert_allclose(g["velocity"].reshape(-1, 3)[idx], d["grid_vel"][gs], rtol=1e-5,
+                                       atol=1e-6 * max(np.abs(d["grid_vel"][gs]).max(), 1.0))
+            np.testing.assert_allclose(g["mass"].reshape(-1)[idx], d["grid_mass"][gs], rtol=1e-5, atol=0)
+        mask = np.ones(g["mass"].size, bool)
+        mask[idx] = False
+        assert np.all(g["mass"].reshape(-1)[mask] == 0)
+
+
+@pytest.mark.parametrize("coupler", ["m45a", "m0"])
+@pytest.mark.parametrize("scene", ["box_drop", "box_drop_dense", "foot_step", "tine_drag", "rover_wheel"])
+def test_sweep_and_dirichlet_research_scenes_match_reference_csv(scene, coupler):
+    """The grid-only research scenes with the M4.5a sweep or M0 Dirichlet
+    coupler (bench_compare_all.cpp, methods "M4.5a" and "M0"): the float32
+    harness loop of tests/m1_scene_loop.py around the CUDA coupler against the
+    reference's shipped *_M4.5a / *_M0 CSVs, to the bars of the M1 scenes."""
+    from tests import m1_scene_loop as L
+    gold = np.load(os.path.join(GOLD, f"{coupler}_scenes.npz"))
+    ref = gold[scene + "_rows"]
+    vals = dict(zip(gold[scene + "_metric_names"], gold[scene + "_metric_values"]))
+    rows = L.run(scene, L.GpuGrid(bm, L.SCENES[scene], coupler))
+    if scene == "tine_drag":
+        fx, fy, n = L.tine_summary(rows)
+        sub = rows[::4]
+        print(f"tine_drag {coupler}: max |dFx| = {np.abs(sub[:, 2] - ref[:, 2]).max():.3e} N, avg draft {fx:.6f} N "
+              f"(reference {vals['avg_draft_fx_n']:.6f})")
+        np.testing.assert_allclose(sub[:, 1], ref[:, 1], rtol=2e-6, atol=1e-6)
+        np.testing.assert_allclose(sub[:, 2:], ref[:, 2:], rtol=1e-5, atol=1e-4)
+        assert n == vals["samples"]
+        assert abs(fx - vals["avg_draft_fx_n"]) <= 1e-5 * abs(vals["avg_draft_fx_n"])
+        return
+    e_pos = np.abs(rows[:, 1:4] - ref[:, 1:4]).max()
+    e_vy = np.abs(rows[:, 4] - ref[:, 4]).max()
+    max_p = np.abs(rows[:, 7]).max()
+    print(f"{scene} {coupler}: max |dx| = {e_pos:.3e} m, max |dvy| = {e_vy:.3e} m/s, max |sum p_y| {max_p:.6f} "
+          f"(reference {vals['max_abs_total_p_y']:.6f})")
+    assert e_pos <= 2e-5
+    assert e_vy <= 2e-4
+    assert np.array_equal(rows[:, 9], ref[:, 9])
+    assert abs(max_p - vals["max_abs_total_p_y"]) <= 1e-4 * vals["max_abs_total_p_y"]
+
+
+def test_dirichlet_unit_tests_on_gpu():
+    """tests/test_mpm_rigid_coupler.cpp:26-92 through the CUDA M0 coupler."""
+    from tests import dirichlet_kats as K
+    for case in K.CASES:
+        s = bm.MPMSolver(0.1, domain=((-8, -8, -8), (40, 40, 40)))
+        s.seed_grid(np.array([case["node"]], np.int32), np.array([case["vel"]], np.float32),
+                    np.array([1.0], np.float32))
+        f, t, n = s.m0_apply(bm.make_collider(**case["body"]), 1.0 / 60.0)
+        g = s.get_grid()
+        o = np.asarray(g["origin"])
+        i, j, k = (np.array(case["node"]) - o)
+        K.check(case, f, t, n, g["velocity"][i, j, k])
+
+
+def test_rigid_drift_dirichlet_matches_reference_csv():
+    """benchmarks/bench_mpm_rigid_drift.cpp with its default method (M0): the
+    unit box over a 5x3x5 patch, 720 steps, against
+    outputs/figures/mpm_rigid_drift.csv (2.6e-7 from the reference rebuilt
+    here, see the oracle pin)."""
+    from tests import m1_scene_loop as L
+    ref = np.load(os.path.join(GOLD, "m0_scenes.npz"))["rigid_drift_rows"]
+    rows = L.run("rigid_drift", L.GpuGrid(bm, L.SCENES["rigid_drift"], "m0"))[:, L.DRIFT_COLUMNS]
+    e_y = np.abs(rows[:, 1] - ref[:, 1]).max()
+    e_vy = np.abs(rows[:, 2] - ref[:, 2]).max()
+    print(f"rigid_drift M0: max |dy| = {e_y:.3e} m, max |dvy| = {e_vy:.3e} m/s")
+    assert e_y <= 2e-5 and e_vy <= 2e-4
+    assert np.array_equal(rows[:, 7], ref[:, 7])
+
+
+@pytest.mark.parametrize("coupler", ["m45a", "m0"])
+def test_sweep_and_dirichlet_coupled_particle_scene_match_reference_split(coupler):
+    """A particle scene with a cylinder stepped by bm_solver_step_coupled with
+    the M4.5a or M0 coupler, against the reference's split phases P2G ->
+    update_grid -> coupler -> G2P."""
+    sc = scenes.wheel_rut(n_keep=20000)
+    body = sc.bodies[0]
+    g = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha, domain=sc.domain)
+    g.set_coupler(coupler)
+    c = cpu_solver(REF, sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+    for n in range(40):
+        b = body.at_time(n * sc.dt)
+        gr = g.step_coupled(sc.dt, [bm.make_collider(**b.as_tuple())])[0]
+        c.p2g(sc.dt)
+        c.grid_update(sc.dt)
+        cr = getattr(c, f"{coupler}_apply")(O.collider(**b.as_tuple()), sc.dt)
+        c.g2p(sc.dt)
+        assert gr[2] == cr[2]
+        np.testing.assert_allclose(gr[0], cr[0], rtol=1e-3, atol=1e-3 * max(1.0, np.abs(cr[0]).max()))
+    e = max_err_dx(g.get_particles()["position"], c.get_particles()["position"], sc.dx)
+    print(f"coupled wheel scene with {coupler}, 40 steps: max |x_gpu - x_ref| = {e:.3e} dx")
+    assert e <= POS_TOL_100
+    assert g.sync() == (0, 0)
 
 
 def _quat_mul(a, b):
