@@ -29,7 +29,7 @@
 //   include/basements/physics/coupling/mpm_rigid_coupler_pic.h:88-184  M1
 //   include/basements/physics/coupling/mpm_rigid_coupler.h:139-200  overlap
 //       fraction and tight world AABB of a shape
-//   research/mpm_rigid_coupling/couplers/m4_5_hybrid.h:104-257  M4.5a
+//   research/mpm_rigid_coupling/couplers/m4_5_hybrid.h:104-305  M4.5a/b/c
 //   include/basements/physics/coupling/mpm_rigid_coupler.h:106-132  outward normal
 //   src/physics/coupling/mpm_rigid_coupler.cpp:58-143  M0 (Dirichlet)
 //   include/basements/physics/dynamics/integrator.h:19-57  rigid update
@@ -484,6 +484,28 @@ template <class R> Reaction<R> m1_apply(Grid<R>& grid, const ColliderF& b, R dt)
     return out;
 }
 
+// mpm_rigid_coupler.h:106-132: outward normal of the closest face in the
+// body frame. Cylinder: the cap (0, +-1, 0) when the axial distance is the
+// smaller, else radial (x/r, 0, z/r), or (1, 0, 0) on the axis. Box: the
+// axis of the smallest face distance, x before y before z on ties.
+template <class R> V3<R> outward_normal_local(const ColliderF& b, const V3<R>& l) {
+    if (b.shape == 1) {
+        const R Rr = (R)b.half_extents[0], L = (R)b.half_extents[1];
+        const R r = std::sqrt(l.x * l.x + l.z * l.z);
+        const R axial = L - std::abs(l.y);
+        const R radial = Rr - r;
+        if (axial < radial) return V3<R>(R(0), l.y >= R(0) ? R(1) : R(-1), R(0));
+        if (r > R(1e-9f)) return V3<R>(l.x / r, R(0), l.z / r);
+        return V3<R>(R(1), R(0), R(0));
+    }
+    const R dx = (R)b.half_extents[0] - std::abs(l.x);
+    const R dy = (R)b.half_extents[1] - std::abs(l.y);
+    const R dz = (R)b.half_extents[2] - std::abs(l.z);
+    if (dx <= dy && dx <= dz) return V3<R>(l.x >= R(0) ? R(1) : R(-1), R(0), R(0));
+    if (dy <= dz) return V3<R>(R(0), l.y >= R(0) ? R(1) : R(-1), R(0));
+    return V3<R>(R(0), R(0), l.z >= R(0) ? R(1) : R(-1));
+}
+
 // mpm_rigid_coupler.h:139-164: 1 at the centre, 0 at the surface; box
 // (1-|x|/hx)(1-|y|/hy)(1-|z|/hz), cylinder (1-|y|/L)(1-r/R), each clamped to [0,1].
 template <class R> R overlap_fraction(const ColliderF& b, const V3<R>& l) {
@@ -517,13 +539,33 @@ template <class R> V3<R> world_aabb_half(const ColliderF& b, const M3<R>& Rl2w) 
                  std::abs(Rl2w.m[2][0]) * hx + std::abs(Rl2w.m[2][1]) * hy + std::abs(Rl2w.m[2][2]) * hz);
 }
 
-// m4_5_hybrid.h:104-212 with the M4_5a rule (:242-257): pass 1 sums the
-// overlap fraction of the nodes inside the shape over the allocated blocks
-// whose node-centre span meets the shape's tight AABB; pass 2 gives each such
-// node m_b = M frac / sum (skipped when m_b <= 0) and the mass-weighted
-// average of node and body velocity (an empty node, mass < 1e-9, takes the
-// body's). The reaction sums m_b (v_after - v_body) / dt and its moment.
-template <class R> Reaction<R> m45a_apply(Grid<R>& grid, const ColliderF& b, R dt) {
+// m4_5_hybrid.h:104-212, the two-pass sweep, with the per-node rule of layer
+// 0 = M4_5a (:242-257), 1 = M4_5b (:259-275), 2 = M4_5c (:282-305): pass 1
+// sums the overlap fraction of the nodes inside the shape over the allocated
+// blocks whose node-centre span meets the shape's tight AABB; pass 2 gives
+// each such node m_b = M frac / sum (skipped when m_b <= 0). Layer c scales
+// m_b by the quadratic B-spline weight of (x_node - centre) / dx (below 1e-6
+// the node takes the body velocity and no mass); every layer takes the
+// mass-weighted average of node and body velocity (an empty node, mass <
+// 1e-9, takes the body's); layers b and c then blend its tangential part
+// toward the body's by min(1, friction) about the closest face's normal. The
+// reaction sums m_b (v_after - v_body) / dt and its moment.
+template <class R> R bspline1d(R xi) {
+    const R a = std::abs(xi);
+    if (a < R(0.5f)) return R(0.75f) - a * a;
+    if (a < R(1.5f)) { const R t = R(1.5f) - a; return R(0.5f) * t * t; }
+    return R(0);
+}
+
+template <class R> V3<R> friction_tangent(const V3<R>& v, const V3<R>& vb, const V3<R>& n, R friction) {
+    const R vn = v.dot(n);
+    const V3<R> vt = v - n * vn;
+    const V3<R> vtb = vb - n * vb.dot(n);
+    const V3<R> vtn = vt + (vtb - vt) * std::min(R(1), friction);
+    return n * vn + vtn;
+}
+
+template <class R> Reaction<R> m45_apply(Grid<R>& grid, const ColliderF& b, R dt, int layer) {
     Reaction<R> out;
     if (dt <= R(0)) return out;
     const R dx = grid.dx;
@@ -560,7 +602,7 @@ template <class R> Reaction<R> m45a_apply(Grid<R>& grid, const ColliderF& b, R d
     const V3<R> w(b.angular_velocity[0], b.angular_velocity[1], b.angular_velocity[2]);
     V3<R> fsum, tsum;
     visit([&](Node<R>& n, const V3<R>& xn, const V3<R>& local) {
-        const R mb = per_frac * overlap_fraction<R>(b, local);
+        R mb = per_frac * overlap_fraction<R>(b, local);
         if (mb <= R(0)) return;
         const V3<R> r = xn - c;
         const V3<R> vb = vl + w.cross(r);
@@ -568,7 +610,26 @@ template <class R> Reaction<R> m45a_apply(Grid<R>& grid, const ColliderF& b, R d
         const R old_m = was_active ? n.m : R(0);
         const V3<R> old_v = was_active ? n.v : V3<R>(R(0));
         V3<R> va = vb;
-        if (was_active) va = (old_v * old_m + vb * mb) / (old_m + mb);
+        bool rule = true;
+        if (layer == 2) {
+            const R k = bspline1d<R>((xn.x - c.x) / dx) * bspline1d<R>((xn.y - c.y) / dx) *
+                        bspline1d<R>((xn.z - c.z) / dx);
+            if (k < R(1e-6f)) {
+                mb = R(0);
+                rule = false;
+            } else {
+                mb = mb * k;
+            }
+        }
+        if (rule) {
+            if (was_active) va = (old_v * old_m + vb * mb) / (old_m + mb);
+            if (layer >= 1) {
+                const V3<R> nw0 = Rl2w * outward_normal_local<R>(b, local);
+                const R len = nw0.length();
+                const V3<R> nw = len < R(1e-6f) ? V3<R>(R(0)) : nw0 / len;
+                va = friction_tangent<R>(va, vb, nw, (R)b.friction);
+            }
+        }
         n.active = true;
         n.m = old_m + mb;
         n.v = va;
@@ -582,26 +643,8 @@ template <class R> Reaction<R> m45a_apply(Grid<R>& grid, const ColliderF& b, R d
     return out;
 }
 
-// mpm_rigid_coupler.h:106-132: outward normal of the closest face in the
-// body frame. Cylinder: the cap (0, +-1, 0) when the axial distance is the
-// smaller, else radial (x/r, 0, z/r), or (1, 0, 0) on the axis. Box: the
-// axis of the smallest face distance, x before y before z on ties.
-template <class R> V3<R> outward_normal_local(const ColliderF& b, const V3<R>& l) {
-    if (b.shape == 1) {
-        const R Rr = (R)b.half_extents[0], L = (R)b.half_extents[1];
-        const R r = std::sqrt(l.x * l.x + l.z * l.z);
-        const R axial = L - std::abs(l.y);
-        const R radial = Rr - r;
-        if (axial < radial) return V3<R>(R(0), l.y >= R(0) ? R(1) : R(-1), R(0));
-        if (r > R(1e-9f)) return V3<R>(l.x / r, R(0), l.z / r);
-        return V3<R>(R(1), R(0), R(0));
-    }
-    const R dx = (R)b.half_extents[0] - std::abs(l.x);
-    const R dy = (R)b.half_extents[1] - std::abs(l.y);
-    const R dz = (R)b.half_extents[2] - std::abs(l.z);
-    if (dx <= dy && dx <= dz) return V3<R>(l.x >= R(0) ? R(1) : R(-1), R(0), R(0));
-    if (dy <= dz) return V3<R>(R(0), l.y >= R(0) ? R(1) : R(-1), R(0));
-    return V3<R>(R(0), R(0), l.z >= R(0) ? R(1) : R(-1));
+template <class R> Reaction<R> m45a_apply(Grid<R>& grid, const ColliderF& b, R dt) {
+    return m45_apply<R>(grid, b, dt, 0);
 }
 
 // mpm_rigid_coupler.cpp:58-143 (M0, Dirichlet): over the allocated blocks

@@ -93,6 +93,8 @@ def load(kind: str):
         "m1_apply": fn("m1_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
         "m45a_apply": fn("m45a_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
         "m0_apply": fn("m0_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
+        "m45b_apply": fn("m45b_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
+        "m45c_apply": fn("m45c_apply", C.c_int, C.c_void_p, C.POINTER(OrcCollider), C.c_float, _f),
         "grid_num_nodes": fn("grid_num_nodes", C.c_int64, C.c_void_p),
         "grid_get": fn("grid_get", C.c_int64, C.c_void_p, _i32, _f, _f, _f, _u8, C.c_int64),
         "grid_seed": fn("grid_seed", None, C.c_void_p, C.c_int64, _i32, _f, _f),
@@ -228,6 +230,19 @@ class CpuSolver:
         r = np.zeros(6, np.float32)
         n = self.api["m0_apply"](self.h, C.byref(body), dt, _p(r))
         return r[:3].copy(), r[3:].copy(), int(n)
+
+    def _coupler(self, name, body, dt):
+        r = np.zeros(6, np.float32)
+        n = self.api[name](self.h, C.byref(body), dt, _p(r))
+        return r[:3].copy(), r[3:].copy(), int(n)
+
+    def m45b_apply(self, body: OrcCollider, dt):
+        """M4.5b: M4.5a plus the friction tangent (m4_5_hybrid.h:259-275)."""
+        return self._coupler("m45b_apply", body, dt)
+
+    def m45c_apply(self, body: OrcCollider, dt):
+        """M4.5 = M4_5c: M4.5b with the B-spline mass weight (m4_5_hybrid.h:282-305)."""
+        return self._coupler("m45c_apply", body, dt)
 
     def m45a_apply(self, body: OrcCollider, dt):
         """The M4.5a two-pass sweep coupler (m4_5_hybrid.h:104-257)."""

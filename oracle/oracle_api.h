@@ -63,6 +63,9 @@ ORC_EXPORT int ORC(m1_apply)(void* h, const orc_collider_t* body, float dt, floa
 ORC_EXPORT int ORC(m0_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
 /* the M4.5a two-pass sweep coupler; same reaction layout */
 ORC_EXPORT int ORC(m45a_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
+/* M4.5b (+ friction tangent) and M4.5 (= M4_5c, + B-spline mass weight) */
+ORC_EXPORT int ORC(m45b_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
+ORC_EXPORT int ORC(m45c_apply)(void* h, const orc_collider_t* body, float dt, float* reaction6);
 ORC_EXPORT int64_t ORC(grid_num_nodes)(void* h);
 /* every node of every allocated block; returns the count written (<= cap) */
 ORC_EXPORT int64_t ORC(grid_get)(void* h, int32_t* ijk, float* vel, float* force, float* mass, uint8_t* active,

@@ -140,6 +140,19 @@ ORC_EXPORT int orc_m0_apply(void* h, const orc_collider_t* body, float dt, float
     return r.nodes_inside;
 }
 
+static int m45_export(void* h, const orc_collider_t* body, float dt, float* reaction6, int layer) {
+    Reaction<R> r = m45_apply<R>(sv(h)->grid, to_collider(body), (R)dt, layer);
+    reaction6[0] = (float)r.force.x; reaction6[1] = (float)r.force.y; reaction6[2] = (float)r.force.z;
+    reaction6[3] = (float)r.torque.x; reaction6[4] = (float)r.torque.y; reaction6[5] = (float)r.torque.z;
+    return r.nodes_inside;
+}
+ORC_EXPORT int orc_m45b_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
+    return m45_export(h, body, dt, reaction6, 1);
+}
+ORC_EXPORT int orc_m45c_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
+    return m45_export(h, body, dt, reaction6, 2);
+}
+
 ORC_EXPORT int orc_m45a_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
     Reaction<R> r = m45a_apply<R>(sv(h)->grid, to_collider(body), (R)dt);
     reaction6[0] = (float)r.force.x; reaction6[1] = (float)r.force.y; reaction6[2] = (float)r.force.z;

@@ -161,6 +161,20 @@ ORC_EXPORT int ref_m0_apply(void* h, const orc_collider_t* body, float dt, float
     return r.nodes_inside;
 }
 
+template <class Coupler>
+static int coupler_export(void* h, const orc_collider_t* body, float dt, float* reaction6) {
+    cp::CouplingReaction r = Coupler::apply(sv(h)->get_grid_mutable(), to_state(body), dt);
+    reaction6[0] = r.force.x; reaction6[1] = r.force.y; reaction6[2] = r.force.z;
+    reaction6[3] = r.torque.x; reaction6[4] = r.torque.y; reaction6[5] = r.torque.z;
+    return r.nodes_inside;
+}
+ORC_EXPORT int ref_m45b_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
+    return coupler_export<research::mpm_rigid::M4_5b>(h, body, dt, reaction6);
+}
+ORC_EXPORT int ref_m45c_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
+    return coupler_export<research::mpm_rigid::M4_5c>(h, body, dt, reaction6);
+}
+
 ORC_EXPORT int ref_m45a_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
     cp::CouplingReaction r = research::mpm_rigid::M4_5a::apply(sv(h)->get_grid_mutable(), to_state(body), dt);
     reaction6[0] = r.force.x; reaction6[1] = r.force.y; reaction6[2] = r.force.z;

@@ -128,8 +128,9 @@ def run_small_scene():
 def m1_cases(n_cases=12, seed=7, coupler="m1_apply"):
     """Seeded grids (empty, tiny and normal node masses) and random box and
     cylinder poses, each through one call of the reference's coupler
-    (MPMRigidCouplerPIC::apply; M4_5a::apply for coupler="m45a_apply";
-    MPMRigidCoupler::apply, M0, for coupler="m0_apply")."""
+    (MPMRigidCouplerPIC::apply; M4_5a/M4_5b/M4_5c::apply for coupler=
+    "m45a_apply"/"m45b_apply"/"m45c_apply"; MPMRigidCoupler::apply, M0, for
+    coupler="m0_apply")."""
     rng = np.random.RandomState(seed)
     out = {k: [] for k in ("dx", "seed_ijk", "seed_vel", "seed_mass", "body", "dt", "force", "torque",
                            "nodes_inside", "grid_ijk", "grid_vel", "grid_mass", "grid_active")}
@@ -258,6 +259,14 @@ def main():
     for scene, summaries in (("box_drop", ("metrics",)),) + M1_SCENES:
         scenes_m0.update(research_csv(a.ref_root, scene, summaries, "M0"))
     np.savez_compressed(os.path.join(HERE, "m0_scenes.npz"), **scenes_m0)
+    for coupler, method, seed in (("m45b", "M4.5b", 37), ("m45c", "M4.5", 41)):
+        np.savez_compressed(os.path.join(HERE, f"{coupler}_cases.npz"), **m1_cases(16, seed, f"{coupler}_apply"))
+        scenes = {}
+        for scene, summaries in (("box_drop", ("metrics",)),) + M1_SCENES:
+            if os.path.exists(os.path.join(a.ref_root, "research/mpm_rigid_coupling/outputs/csv",
+                                           f"{scene}_{method}.csv")):
+                scenes.update(research_csv(a.ref_root, scene, summaries, method))
+        np.savez_compressed(os.path.join(HERE, f"{coupler}_scenes.npz"), **scenes)
     np.savez_compressed(os.path.join(HERE, "svd_cases.npz"), **svd_cases())
     np.savez_compressed(os.path.join(HERE, "constitutive.npz"), **constitutive())
     for f in sorted(os.listdir(HERE)):
