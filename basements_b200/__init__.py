@@ -138,6 +138,8 @@ _SIGS = {
     "bm_coupler_m1_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
     "bm_coupler_m45a_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
     "bm_coupler_m0_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
+    "bm_coupler_m45b_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
+    "bm_coupler_m45_apply": (_st, [_h, C.POINTER(Collider), C.c_float, C.POINTER(Reaction)]),
     "bm_solver_set_coupler": (_st, [_h, C.c_int32]),
     "bm_solver_g2p": (_st, [_h, C.c_float]),
     "bm_solver_step_coupled": (_st, [_h, C.c_float, C.c_int32, C.POINTER(Collider), C.POINTER(Reaction)]),
@@ -382,9 +384,23 @@ class MPMSolver:
         check(lib().bm_coupler_m0_apply(self._h, C.byref(body), dt, C.byref(r)), "bm_coupler_m0_apply")
         return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
 
+    def m45b_apply(self, body: Collider, dt):
+        """The M4.5b sweep layer (M4.5a + friction tangent)."""
+        r = Reaction()
+        check(lib().bm_coupler_m45b_apply(self._h, C.byref(body), dt, C.byref(r)), "bm_coupler_m45b_apply")
+        return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
+
+    def m45c_apply(self, body: Collider, dt):
+        """The M4.5 sweep layer (M4_5c: M4.5b + B-spline mass weight)."""
+        r = Reaction()
+        check(lib().bm_coupler_m45_apply(self._h, C.byref(body), dt, C.byref(r)), "bm_coupler_m45_apply")
+        return np.array(r.force[:], np.float32), np.array(r.torque[:], np.float32), int(r.nodes_inside)
+
+    COUPLERS = {"m1": 0, "m45a": 1, "m0": 2, "m45b": 3, "m45c": 4}
+
     def set_coupler(self, name: str):
-        """Coupler of step_coupled: "m1" (default), "m45a" or "m0"."""
-        check(lib().bm_solver_set_coupler(self._h, {"m1": 0, "m45a": 1, "m0": 2}[name]), "bm_solver_set_coupler")
+        """Coupler of step_coupled: "m1" (default), "m45a", "m45b", "m45c" (M4.5) or "m0"."""
+        check(lib().bm_solver_set_coupler(self._h, self.COUPLERS[name]), "bm_solver_set_coupler")
 
     def step_coupled(self, dt, bodies, read_reactions=True):
         n = len(bodies)

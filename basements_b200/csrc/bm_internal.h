@@ -266,11 +266,12 @@ void launch_m0(const SceneTable& t, const M1Params* d_param, int64_t candidates,
 // M4.5a frame of one body of scene 0: the shape's tight AABB in lo/hi, the
 // body's mass in mb.
 bool m45a_prepare(const GridDesc& g, const bm_collider_t& b, float dt, M1Params* out);
-// The two passes of M4.5a for one body over `candidates` blocks (P.nbi *
-// P.nbj * P.nbk): Sigma frac into *d_frac_sum (zeroed by the caller), then the
-// exchange, reaction added into d_acc (7 doubles, zeroed by the caller).
-void launch_m45a(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt,
-                 double* d_frac_sum, double* d_acc, cudaStream_t st);
+// The two passes of the sweep couplers for one body over `candidates` blocks
+// (P.nbi * P.nbj * P.nbk): Sigma frac into *d_frac_sum (zeroed by the
+// caller), then the exchange with the rule of layer 0 = M4.5a, 1 = M4.5b,
+// 2 = M4.5, reaction added into d_acc (7 doubles, zeroed by the caller).
+void launch_m45(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt,
+                double* d_frac_sum, double* d_acc, int layer, cudaStream_t st);
 // True when the candidate block ranges of two bodies of one scene intersect
 // (they may then write the same nodes).
 inline bool m1_blocks_overlap(const M1Params& a, const M1Params& b) {

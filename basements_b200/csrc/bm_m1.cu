@@ -187,6 +187,43 @@ __device__ __forceinline__ float dot3(const float a[3], const float b[3]) {
     return add(add(mul(a[0], b[0]), mul(a[1], b[1])), mul(a[2], b[2]));
 }
 
+// (R_l2w * shape_outward_normal_local).normalized() (Vec3::normalized: zero
+// below length 1e-6).
+__device__ __forceinline__ void world_face_normal(const M1Params& P, const float l[3], float nw[3]) {
+    float nl[3];
+    outward_normal_local(P, l, nl);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        nw[a] = add(add(mul(P.R[3 * a], nl[0]), mul(P.R[3 * a + 1], nl[1])), mul(P.R[3 * a + 2], nl[2]));
+    const float len = __fsqrt_rn(dot3(nw, nw));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) nw[a] = len < 1e-6f ? 0.0f : dvd(nw[a], len);
+}
+
+// apply_friction_tangent (m4_5_hybrid.h:225-232): keep the normal part of v,
+// blend its tangential part toward the body's by min(1, friction).
+__device__ __forceinline__ void friction_tangent(float v[3], const float vb[3], const float n[3], float friction) {
+    const float vn = dot3(v, n), vbn = dot3(vb, n);
+    const float fr = friction < 1.0f ? friction : 1.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float vt = sub(v[a], mul(n[a], vn));
+        const float vtb = sub(vb[a], mul(n[a], vbn));
+        v[a] = add(mul(n[a], vn), add(vt, mul(sub(vtb, vt), fr)));
+    }
+}
+
+// bspline1d (m4_5_hybrid.h:58-63): the quadratic B-spline, 0 beyond 1.5.
+__device__ __forceinline__ float bspline1d(float xi) {
+    const float a = fabsf(xi);
+    if (a < 0.5f) return sub(0.75f, mul(a, a));
+    if (a < 1.5f) {
+        const float t = sub(1.5f, a);
+        return mul(mul(0.5f, t), t);
+    }
+    return 0.0f;
+}
+
 // M0, MPMRigidCoupler::apply (mpm_rigid_coupler.cpp:58-143): over the
 // visited blocks of the M1 frame, a node with mass > 1e-8 inside the shape
 // keeps its normal velocity no slower outward than the body's (n = the
@@ -216,14 +253,8 @@ __global__ void __launch_bounds__(64) k_m0(SceneTable t, const M1Params* params,
             const float vb[3] = {add(P.vl[0], sub(mul(P.w[1], r[2]), mul(P.w[2], r[1]))),
                                  add(P.vl[1], sub(mul(P.w[2], r[0]), mul(P.w[0], r[2]))),
                                  add(P.vl[2], sub(mul(P.w[0], r[1]), mul(P.w[1], r[0])))};
-            float nl[3], nw[3];
-            outward_normal_local(P, l, nl);
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-                nw[a] = add(add(mul(P.R[3 * a], nl[0]), mul(P.R[3 * a + 1], nl[1])), mul(P.R[3 * a + 2], nl[2]));
-            const float len = __fsqrt_rn(dot3(nw, nw));
-#pragma unroll
-            for (int a = 0; a < 3; ++a) nw[a] = len < 1e-6f ? 0.0f : dvd(nw[a], len);
+            float nw[3];
+            world_face_normal(P, l, nw);
             const float v[3] = {nv.x, nv.y, nv.z};
             const float vn_node = dot3(v, nw), vn_body = dot3(vb, nw);
             const float vn_cl = vn_node < vn_body ? vn_body : vn_node;
@@ -275,13 +306,18 @@ __global__ void __launch_bounds__(64) k_m45a_sum(SceneTable t, const M1Params* p
     cta64_add<1>(vals, frac_sum);
 }
 
-// M4.5a pass 2 (m4_5_hybrid.h:148-208 with the M4_5a rule :242-257): each
-// inside node gets m_b = M frac / sum (skipped when m_b <= 0) and the
-// mass-weighted average of node and body velocity, as in M1; reaction into
-// acc (force, torque, count) per CTA in double. The sum arrives in double and
-// is used in float, the type of the reference's accumulator.
-__global__ void __launch_bounds__(64) k_m45a(SceneTable t, const M1Params* params, int cur, float dt,
-                                             const double* frac_sum, double* acc) {
+// Sweep pass 2 (m4_5_hybrid.h:148-208) with the rule of Layer 0 = M4_5a
+// (:242-257), 1 = M4_5b (:259-275), 2 = M4_5c (:282-305): each inside node
+// gets m_b = M frac / sum (skipped when m_b <= 0; layer c scales it by the
+// B-spline weight of (x_node - centre) / dx and, below 1e-6, gives the node
+// the body velocity and no mass) and the mass-weighted average of node and
+// body velocity, as in M1; layers b and c then blend its tangential part
+// toward the body's about the closest face's normal. Reaction into acc
+// (force, torque, count) per CTA in double. The sum arrives in double and is
+// used in float, the type of the reference's accumulator.
+template <int Layer>
+__global__ void __launch_bounds__(64) k_m45(SceneTable t, const M1Params* params, int cur, float dt,
+                                            const double* frac_sum, double* acc) {
     const M1Params& P = params[0];
     if (!P.active) return;
     const int64_t cb = blockIdx.x;
@@ -301,21 +337,29 @@ __global__ void __launch_bounds__(64) k_m45a(SceneTable t, const M1Params* param
         float r[3], l[3];
         if (coupler_node_local(P, g.dx, g.ox + 4 * bi + (tt >> 4), g.oy + 4 * bj + ((tt >> 2) & 3),
                                g.oz + 4 * bk + (tt & 3), r, l)) {
-            const float mb = mul(per_frac, coupler_overlap_fraction(P, l));
+            float mb = mul(per_frac, coupler_overlap_fraction(P, l));
             if (!(mb <= 0.0f)) {
                 const float vb[3] = {add(P.vl[0], sub(mul(P.w[1], r[2]), mul(P.w[2], r[1]))),
                                      add(P.vl[1], sub(mul(P.w[2], r[0]), mul(P.w[0], r[2]))),
                                      add(P.vl[2], sub(mul(P.w[0], r[1]), mul(P.w[1], r[0])))};
+                bool rule = true;
+                if (Layer == 2) {
+                    const float k = mul(mul(bspline1d(dvd(r[0], g.dx)), bspline1d(dvd(r[1], g.dx))),
+                                        bspline1d(dvd(r[2], g.dx)));
+                    if (k < 1e-6f) {
+                        mb = 0.0f;
+                        rule = false;
+                    } else {
+                        mb = mul(mb, k);
+                    }
+                }
                 const int64_t id = g.node_of_block(blin, tt);
                 float4 nv = A.mv[id];
                 float4 nf = A.f[id];
                 const float m_tot = node_total_mass(nv, nf);
-                float va[3];
-                if (!(m_tot >= 1e-9f)) {  // inactive or below kInactiveNodeMassEpsilon: the body's velocity
-                    va[0] = vb[0]; va[1] = vb[1]; va[2] = vb[2];
-                    nv = make_float4(vb[0], vb[1], vb[2], 0.0f);
-                    nf.w = mb;
-                } else {
+                float va[3] = {vb[0], vb[1], vb[2]};
+                const bool was_active = m_tot >= 1e-9f;  // else the node's mass is dropped (old_mass = 0)
+                if (rule && was_active) {
                     const float mn = add(m_tot, mb);
                     const float pa[3] = {add(mul(nv.x, m_tot), mul(vb[0], mb)), add(mul(nv.y, m_tot), mul(vb[1], mb)),
                                          add(mul(nv.z, m_tot), mul(vb[2], mb))};
@@ -324,9 +368,14 @@ __global__ void __launch_bounds__(64) k_m45a(SceneTable t, const M1Params* param
                     } else {
                         va[0] = dvd(pa[0], mn); va[1] = dvd(pa[1], mn); va[2] = dvd(pa[2], mn);
                     }
-                    nv = make_float4(va[0], va[1], va[2], nv.w);
-                    nf.w = mn;
                 }
+                if (Layer >= 1 && rule) {
+                    float nw[3];
+                    world_face_normal(P, l, nw);
+                    friction_tangent(va, vb, nw, P.friction);
+                }
+                nv = make_float4(va[0], va[1], va[2], was_active ? nv.w : 0.0f);
+                nf.w = was_active ? add(m_tot, mb) : mb;
                 A.mv[id] = nv;
                 A.f[id] = nf;
                 touch_block(A, blin);
@@ -558,11 +607,13 @@ void launch_m0(const SceneTable& t, const M1Params* d_param, int64_t candidates,
     k_m0<<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, dt, d_acc);
 }
 
-void launch_m45a(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt,
-                 double* d_frac_sum, double* d_acc, cudaStream_t st) {
+void launch_m45(const SceneTable& t, const M1Params* d_param, int64_t candidates, int cur, float dt,
+                double* d_frac_sum, double* d_acc, int layer, cudaStream_t st) {
     if (candidates <= 0) return;
     k_m45a_sum<<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, d_frac_sum);
-    k_m45a<<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, dt, d_frac_sum, d_acc);
+    if (layer == 2) k_m45<2><<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, dt, d_frac_sum, d_acc);
+    else if (layer == 1) k_m45<1><<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, dt, d_frac_sum, d_acc);
+    else k_m45<0><<<(unsigned)candidates, 64, 0, st>>>(t, d_param, cur, dt, d_frac_sum, d_acc);
 }
 
 int64_t m1_max_candidates(const GridDesc& g, const float he[3]) {

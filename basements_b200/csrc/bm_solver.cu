@@ -155,7 +155,7 @@ bm_status_t do_m0(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float
 
 // The reference applies a coupler to one body at a time (ApplyFn,
 // bench_compare_all.cpp:50-51); each body's two passes run in order.
-bm_status_t do_m45a(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt) {
+bm_status_t do_m45(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt, int layer) {
     bm_status_t st = ensure_reactions(s, std::max(1, n_bodies));
     if (st != BM_OK) return st;
     s->h_params.resize(n_bodies);
@@ -166,17 +166,17 @@ bm_status_t do_m45a(bm_solver* s, int n_bodies, const bm_collider_t* bodies, flo
     if (n_bodies > 0)
         BM_CHECK_CUDA(cudaMemcpyAsync(s->d_params, hp.data(), sizeof(M1Params) * n_bodies, cudaMemcpyHostToDevice,
                                       s->w.stream));
-    s->w.timed("m45a_coupler", [&] {
+    s->w.timed("m45_coupler", [&] {
         for (int b = 0; b < n_bodies; ++b) {
             const M1Params& P = hp[b];
             if (!P.active) continue;
-            launch_m45a(s->w.table(), s->d_params + b, (int64_t)P.nbi * P.nbj * P.nbk, s->w.cur, dt,
-                        s->d_frac_sum + b, s->d_acc + 7 * b, s->w.stream);
+            launch_m45(s->w.table(), s->d_params + b, (int64_t)P.nbi * P.nbj * P.nbk, s->w.cur, dt,
+                       s->d_frac_sum + b, s->d_acc + 7 * b, layer, s->w.stream);
         }
     });
     launch_reaction_finalize(s->d_acc, n_bodies, s->d_react, s->w.stream);
     s->view = s->w.cur;
-    return launch_status("m45a");
+    return launch_status("m45");
 }
 
 bm_status_t do_g2p(bm_solver* s, float dt) {
@@ -220,9 +220,11 @@ bm_status_t do_step(bm_solver* s, float dt, int32_t n_bodies, const bm_collider_
     if (st == BM_OK && !s->acc_valid) st = do_p2g(s);
     if (st == BM_OK) st = do_grid_update(s, dt);
     if (st == BM_OK && n_bodies > 0)
-        st = s->coupler == BM_COUPLER_M45A ? do_m45a(s, n_bodies, bodies, dt)
-             : s->coupler == BM_COUPLER_M0 ? do_m0(s, n_bodies, bodies, dt)
-                                           : do_m1(s, n_bodies, bodies, dt);
+        st = s->coupler == BM_COUPLER_M45A   ? do_m45(s, n_bodies, bodies, dt, 0)
+             : s->coupler == BM_COUPLER_M45B ? do_m45(s, n_bodies, bodies, dt, 1)
+             : s->coupler == BM_COUPLER_M45  ? do_m45(s, n_bodies, bodies, dt, 2)
+             : s->coupler == BM_COUPLER_M0   ? do_m0(s, n_bodies, bodies, dt)
+                                             : do_m1(s, n_bodies, bodies, dt);
     if (st == BM_OK) st = do_g2p2g(s, dt);
     return st;
 }
@@ -549,14 +551,25 @@ BM_API bm_status_t bm_coupler_m0_apply(bm_solver_t* s, const bm_collider_t* body
     return coupler_call(s, body, dt, out, &do_m0);
 }
 
+bm_status_t do_m45a(bm_solver* s, int n, const bm_collider_t* b, float dt) { return do_m45(s, n, b, dt, 0); }
+bm_status_t do_m45b(bm_solver* s, int n, const bm_collider_t* b, float dt) { return do_m45(s, n, b, dt, 1); }
+bm_status_t do_m45c(bm_solver* s, int n, const bm_collider_t* b, float dt) { return do_m45(s, n, b, dt, 2); }
+
 BM_API bm_status_t bm_coupler_m45a_apply(bm_solver_t* s, const bm_collider_t* body, float dt, bm_reaction_t* out) {
     return coupler_call(s, body, dt, out, &do_m45a);
 }
 
+BM_API bm_status_t bm_coupler_m45b_apply(bm_solver_t* s, const bm_collider_t* body, float dt, bm_reaction_t* out) {
+    return coupler_call(s, body, dt, out, &do_m45b);
+}
+
+BM_API bm_status_t bm_coupler_m45_apply(bm_solver_t* s, const bm_collider_t* body, float dt, bm_reaction_t* out) {
+    return coupler_call(s, body, dt, out, &do_m45c);
+}
+
 BM_API bm_status_t bm_solver_set_coupler(bm_solver_t* s, int32_t coupler) {
     if (!s) return invalid_arg("NULL handle");
-    if (coupler != BM_COUPLER_M1 && coupler != BM_COUPLER_M45A && coupler != BM_COUPLER_M0)
-        return invalid_arg("unknown coupler");
+    if (coupler < BM_COUPLER_M1 || coupler > BM_COUPLER_M45) return invalid_arg("unknown coupler");
     s->coupler = coupler;
     return BM_OK;
 }

@@ -60,8 +60,9 @@ bm_status_t do_grid_update(bm_solver* s, float dt);
 bm_status_t do_m1(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt);
 // M0 for each body in order on acc[cur]; reactions into s->d_react.
 bm_status_t do_m0(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt);
-// M4.5a for each body in order on acc[cur]; reactions into s->d_react.
-bm_status_t do_m45a(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt);
+// The sweep coupler of layer 0 = M4.5a, 1 = M4.5b, 2 = M4.5 for each body in
+// order on acc[cur]; reactions into s->d_react.
+bm_status_t do_m45(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float dt, int layer);
 // The standalone G2P from acc[cur].
 bm_status_t do_g2p(bm_solver* s, float dt);
 // The particle order or grid contents changed behind the solver's back.

@@ -199,13 +199,26 @@ BM_API bm_status_t bm_coupler_m45a_apply(bm_solver_t* s, const bm_collider_t* bo
  * matches the reference bit for bit, the reaction to its summation order. */
 BM_API bm_status_t bm_coupler_m0_apply(bm_solver_t* s, const bm_collider_t* body, float dt,
                                        bm_reaction_t* out);
+/* The other two layers of the sweep (m4_5_hybrid.h): M4.5b, M4_5b::apply
+ * (:259-275), adds to M4.5a the Coulomb tangent projection (the node's
+ * tangential velocity about the closest face's normal blended toward the
+ * body's by min(1, friction)); M4.5, M4_5c::apply (:282-305), also scales
+ * each node's mass share by the quadratic B-spline weight of its offset from
+ * the centre, which by design breaks sum m_b = M. Same contract and
+ * precision as bm_coupler_m45a_apply. */
+BM_API bm_status_t bm_coupler_m45b_apply(bm_solver_t* s, const bm_collider_t* body, float dt,
+                                         bm_reaction_t* out);
+BM_API bm_status_t bm_coupler_m45_apply(bm_solver_t* s, const bm_collider_t* body, float dt,
+                                        bm_reaction_t* out);
 /* Coupler that bm_solver_step_coupled applies to its bodies (each body in
  * order, the ApplyFn table of bench_compare_all.cpp:50-70): BM_COUPLER_M1
- * (default), BM_COUPLER_M45A or BM_COUPLER_M0. The batched and served forms
- * and the tape use M1. */
+ * (default), BM_COUPLER_M45A, BM_COUPLER_M0, BM_COUPLER_M45B or
+ * BM_COUPLER_M45. The batched and served forms and the tape use M1. */
 #define BM_COUPLER_M1 0
 #define BM_COUPLER_M45A 1
 #define BM_COUPLER_M0 2
+#define BM_COUPLER_M45B 3
+#define BM_COUPLER_M45 4
 BM_API bm_status_t bm_solver_set_coupler(bm_solver_t* s, int32_t coupler);
 /* The G2P loop (:83-86). */
 BM_API bm_status_t bm_solver_g2p(bm_solver_t* s, float dt);

@@ -64,11 +64,11 @@ def test_m1_matches_reference_fixtures():
         assert np.all(g["mass"].reshape(-1)[mask] == 0)
 
 
-@pytest.mark.parametrize("coupler", ["m45a", "m0"])
+@pytest.mark.parametrize("coupler", ["m45a", "m45b", "m45c", "m0"])
 def test_sweep_and_dirichlet_match_reference_fixtures(coupler):
     """One call of the CUDA M4.5a sweep or M0 Dirichlet coupler on the seeded
-    grids of m45a_cases.npz / m0_cases.npz (made by the reference's
-    M4_5a::apply / MPMRigidCoupler::apply). nodes_inside exactly; force and
+    grids of m45a/m45b/m45c_cases.npz / m0_cases.npz (made by the reference's
+    M4_5a/M4_5b/M4_5c::apply / MPMRigidCoupler::apply). nodes_inside exactly; force and
     torque to 1e-5 of their largest component (summed in double per CTA, in
     float in hash-map order by the reference). M0's node update is per node,
     so its grid is exact; M4.5a's overlap sum is taken in double on the
@@ -103,13 +103,24 @@ def test_sweep_and_dirichlet_match_reference_fixtures(coupler):
         assert np.all(g["mass"].reshape(-1)[mask] == 0)
 
 
-@pytest.mark.parametrize("coupler", ["m45a", "m0"])
-@pytest.mark.parametrize("scene", ["box_drop", "box_drop_dense", "foot_step", "tine_drag", "rover_wheel"])
-def test_sweep_and_dirichlet_research_scenes_match_reference_csv(scene, coupler):
-    """The grid-only research scenes with the M4.5a sweep or M0 Dirichlet
-    coupler (bench_compare_all.cpp, methods "M4.5a" and "M0"): the float32
-    harness loop of tests/m1_scene_loop.py around the CUDA coupler against the
-    reference's shipped *_M4.5a / *_M0 CSVs, to the bars of the M1 scenes."""
+def _scene_cases():
+    """(coupler, scene) pairs with a shipped CSV (no tine_drag for M4.5)."""
+    out = []
+    for coupler in ("m45a", "m45b", "m45c", "m0"):
+        d = np.load(os.path.join(GOLD, f"{coupler}_scenes.npz"))
+        out += [(coupler, s) for s in ("box_drop", "box_drop_dense", "foot_step", "tine_drag", "rover_wheel")
+                if f"{s}_rows" in d.files]
+    return out
+
+
+@pytest.mark.parametrize("coupler,scene", _scene_cases())
+def test_sweep_and_dirichlet_research_scenes_match_reference_csv(coupler, scene):
+    """The grid-only research scenes with the sweep couplers or M0
+    (bench_compare_all.cpp, methods "M4.5a", "M4.5b", "M4.5" and "M0"): the
+    float32 harness loop of tests/m1_scene_loop.py around the CUDA coupler
+    against the reference's shipped CSVs, to the bars of the M1 scenes
+    (relative to the size of the positions and velocities for the M4.5
+    rover, whose wheel falls 30 m through the sand)."""
     from tests import m1_scene_loop as L
     gold = np.load(os.path.join(GOLD, f"{coupler}_scenes.npz"))
     ref = gold[scene + "_rows"]
@@ -130,8 +141,8 @@ def test_sweep_and_dirichlet_research_scenes_match_reference_csv(scene, coupler)
     max_p = np.abs(rows[:, 7]).max()
     print(f"{scene} {coupler}: max |dx| = {e_pos:.3e} m, max |dvy| = {e_vy:.3e} m/s, max |sum p_y| {max_p:.6f} "
           f"(reference {vals['max_abs_total_p_y']:.6f})")
-    assert e_pos <= 2e-5
-    assert e_vy <= 2e-4
+    assert e_pos <= 2e-5 * max(1.0, np.abs(ref[:, 1:4]).max())
+    assert e_vy <= 2e-4 * max(1.0, np.abs(ref[:, 4]).max())
     assert np.array_equal(rows[:, 9], ref[:, 9])
     assert abs(max_p - vals["max_abs_total_p_y"]) <= 1e-4 * vals["max_abs_total_p_y"]
 
@@ -179,7 +190,7 @@ def test_rigid_drift_dirichlet_matches_reference_csv():
     assert np.array_equal(rows[:, 7], ref[:, 7])
 
 
-@pytest.mark.parametrize("coupler", ["m45a", "m0"])
+@pytest.mark.parametrize("coupler", ["m45a", "m45b", "m45c", "m0"])
 def test_sweep_and_dirichlet_coupled_particle_scene_match_reference_split(coupler):
     """A particle scene with a cylinder stepped by bm_solver_step_coupled with
     the M4.5a or M0 coupler, against the reference's split phases P2G ->
