@@ -523,6 +523,7 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
         if (inside) {
             float4* dmv = next.mv + g.node_rel(r0, r1, r2);
             float4* df = next.f + g.node_rel(r0, r1, r2);
+            uint32_t light = 0u;  // bit 9i+3j+k: w m <= 1e-6 at that node
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 // m v + (m C + dt S) d, summed axis by axis
@@ -542,14 +543,23 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
                         const int64_t off = i * EYZ + j * EZ + k;
                         red_v4(dmv + off, (uj[0] + Mq[2] * dd[2][k]) * w, (uj[1] + Mq[5] * dd[2][k]) * w,
                                (uj[2] + Mq[8] * dd[2][k]) * w, mc);
-                        if (mc <= 1e-6f && !(heavy & (1u << (9 * i + 3 * j + k)))) {
-                            const float d0 = dd[0][i], d1 = dd[1][j], d2 = dd[2][k];
-                            red_v4(df + off, ((sk[0] * d0 + sk[1] * d1) + sk[2] * d2) * w,
-                                   ((sk[3] * d0 + sk[4] * d1) + sk[5] * d2) * w,
-                                   ((sk[6] * d0 + sk[7] * d1) + sk[8] * d2) * w, 0.0f);
-                        }
+                        if (mc <= 1e-6f) light |= 1u << (9 * i + 3 * j + k);
                     }
                 }
+            }
+            // the force records of light contributions at nodes that were not
+            // heavy, off the unrolled loop (few per particle)
+            light &= ~heavy;
+#pragma unroll 1
+            while (light) {
+                const int n = __ffs(light) - 1;
+                light &= light - 1;
+                const int i = n / 9, j = (n / 3) % 3, k = n % 3;
+                const float w = pick3(wgt[0], i) * pick3(wgt[1], j) * pick3(wgt[2], k);
+                const float d0 = pick3(dd[0], i), d1 = pick3(dd[1], j), d2 = pick3(dd[2], k);
+                red_v4(df + (i * EYZ + j * EZ + k), ((sk[0] * d0 + sk[1] * d1) + sk[2] * d2) * w,
+                       ((sk[3] * d0 + sk[4] * d1) + sk[5] * d2) * w, ((sk[6] * d0 + sk[7] * d1) + sk[8] * d2) * w,
+                       0.0f);
             }
         } else {
 #pragma unroll 1
