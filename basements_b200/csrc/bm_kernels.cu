@@ -827,6 +827,7 @@ struct FusedVariant {
     {#T "x" #B, T, {k_g2p2g<false, T, B>, k_g2p2g<true, T, B>}, {k_g2p2g_one<false, T, B>, k_g2p2g_one<true, T, B>}}
 const FusedVariant kFused[] = {
     BM_FUSED(128, 4), BM_FUSED(128, 5), BM_FUSED(128, 6), BM_FUSED(256, 2), BM_FUSED(256, 3), BM_FUSED(64, 10),
+    BM_FUSED(128, 8), BM_FUSED(128, 7),
 };
 #undef BM_FUSED
 constexpr int kNumFused = sizeof(kFused) / sizeof(kFused[0]);
