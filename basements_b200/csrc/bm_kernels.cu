@@ -51,6 +51,10 @@ __device__ __forceinline__ void red_v4(float4* a, float x, float y, float z, flo
                  : "memory");
 }
 
+// Largest CTA of the fused kernel's launch shapes (its per-thread shared
+// columns are sized for it).
+constexpr int kMaxFusedThreads = 256;
+
 // a[i] for a runtime i in {0,1,2} without indexing (keeps `a` in registers).
 __device__ __forceinline__ float pick3(const float a[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
 
@@ -504,6 +508,12 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
     for (int q = 0; q < 9; ++q) Mq[q] = m * Cm[q] + dt * sk[q];
 #pragma unroll
     for (int a = 0; a < 3; ++a) Pm[a] = m * v[a];
+    // S itself is needed again only for the (few) light-force records after
+    // the unrolled scatter: park it in this thread's shared-memory column so
+    // that it holds no registers through the loop
+    __shared__ float sk_park[9 * kMaxFusedThreads];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) sk_park[q * kMaxFusedThreads + threadIdx.x] = sk[q];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         fx[a] = x[a] * g.inv_dx - 0.5f;
@@ -557,8 +567,11 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
                 const int i = n / 9, j = (n / 3) % 3, k = n % 3;
                 const float w = pick3(wgt[0], i) * pick3(wgt[1], j) * pick3(wgt[2], k);
                 const float d0 = pick3(dd[0], i), d1 = pick3(dd[1], j), d2 = pick3(dd[2], k);
-                red_v4(df + (i * EYZ + j * EZ + k), ((sk[0] * d0 + sk[1] * d1) + sk[2] * d2) * w,
-                       ((sk[3] * d0 + sk[4] * d1) + sk[5] * d2) * w, ((sk[6] * d0 + sk[7] * d1) + sk[8] * d2) * w,
+                float S_[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) S_[q] = sk_park[q * kMaxFusedThreads + threadIdx.x];
+                red_v4(df + (i * EYZ + j * EZ + k), ((S_[0] * d0 + S_[1] * d1) + S_[2] * d2) * w,
+                       ((S_[3] * d0 + S_[4] * d1) + S_[5] * d2) * w, ((S_[6] * d0 + S_[7] * d1) + S_[8] * d2) * w,
                        0.0f);
             }
         } else {
@@ -574,10 +587,14 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
                 red_v4(next.mv + id, (Pm[0] + ((Mq[0] * d0 + Mq[1] * d1) + Mq[2] * d2)) * w,
                        (Pm[1] + ((Mq[3] * d0 + Mq[4] * d1) + Mq[5] * d2)) * w,
                        (Pm[2] + ((Mq[6] * d0 + Mq[7] * d1) + Mq[8] * d2)) * w, mc);
-                if (mc <= 1e-6f)
-                    red_v4(next.f + id, ((sk[0] * d0 + sk[1] * d1) + sk[2] * d2) * w,
-                           ((sk[3] * d0 + sk[4] * d1) + sk[5] * d2) * w, ((sk[6] * d0 + sk[7] * d1) + sk[8] * d2) * w,
+                if (mc <= 1e-6f) {
+                    float S_[9];
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) S_[q] = sk_park[q * kMaxFusedThreads + threadIdx.x];
+                    red_v4(next.f + id, ((S_[0] * d0 + S_[1] * d1) + S_[2] * d2) * w,
+                           ((S_[3] * d0 + S_[4] * d1) + S_[5] * d2) * w, ((S_[6] * d0 + S_[7] * d1) + S_[8] * d2) * w,
                            0.0f);
+                }
             }
         }
     }
