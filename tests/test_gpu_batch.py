@@ -6,6 +6,8 @@ match the reference's own solver, coupler and rigid integrator run alone on
 the CPU (oracle/_ref run_dynamic_body: P2G, update_grid, M1 on the body's
 current state, TimeIntegrator, G2P), to the accuracy bar of the plain step.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -55,6 +57,29 @@ def test_batch_of_one_equals_plain_solver():
     b.step(50)
     g.step(sc.dt, 50)
     assert max_err_dx(b.get_particles(0)["position"], g.get_particles()["position"], sc.dx) < 1e-5
+
+
+def test_ragged_batch_with_empty_and_single_particle_scenes():
+    """An empty scene (explicit box, no particles), a one-particle scene and a
+    sand column step together, eagerly and through graph chunks: the empty
+    scene stays empty and the others equal the plain solver run alone."""
+    col = scenes.sand_column(cells=(8, 6, 8))
+    empty = dataclasses.replace(col, name="empty", position=np.zeros((0, 3), np.float32),
+                                mass=np.zeros(0, np.float32), domain=((0, 0, 0), (32, 32, 32)))
+    one = dataclasses.replace(col, name="one", position=col.position[:1].copy(), mass=col.mass[:1].copy())
+    steps = 2 * 16 + 7  # eager head, graph chunks, eager tail
+    b = bm.Batch([empty, one, col, empty])
+    b.step(steps)
+    st, scene, esc = b.sync()
+    assert (st, esc) == (0, 0), scene
+    assert b.num_particles(0) == 0 and b.num_particles(3) == 0
+    assert b.get_particles(0)["position"].shape == (0, 3)
+    for i, sc in ((1, one), (2, col)):
+        g = gpu_solver(sc.dx, sc.position, None, sc.mass, sc.E, sc.nu, sc.rho, sc.alpha)
+        g.step(sc.dt, steps)
+        e = max_err_dx(b.get_particles(i)["position"], g.get_particles()["position"], sc.dx)
+        print(f"scene {i} ({sc.n} particles): max |x_batch - x_plain| = {e:.2e} dx")
+        assert e < 1e-5, i
 
 
 def test_graph_replay_equals_eager_steps():
