@@ -660,7 +660,7 @@ BM_API bm_status_t bm_server_result(bm_server_t* s, int64_t id, const bm_particl
         return BM_ERR_STATE;
     }
     const size_t n = r.mass.size();
-    if (v) {
+    if (v && n > 0) {
         if (v->position) std::memcpy(v->position, r.out_pos.data(), sizeof(float) * 3 * n);
         if (v->velocity) std::memcpy(v->velocity, r.out_vel.data(), sizeof(float) * 3 * n);
         if (v->F) std::memcpy(v->F, r.out_F.data(), sizeof(float) * 9 * n);

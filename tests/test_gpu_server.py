@@ -10,6 +10,7 @@ step missed, taken twice or taken with another scene's state moves the sand
 by ~1e-2 dx. It must also match the reference's own
 solver, coupler and integrator run alone on the CPU.
 """
+import dataclasses
 import time
 
 import numpy as np
@@ -75,6 +76,38 @@ def test_admission_respects_the_hbm_budget():
     assert st["completed"] == 4 and st["peak_bytes"] <= 1.5 * one
     with pytest.raises(bm.BMError):
         srv.submit(req_scene(60, 60000), 5)  # larger than the whole budget
+    srv.close()
+
+
+def test_failing_request_is_isolated_and_edge_requests():
+    """A request whose sand leaves its box completes with BM_ERR_DOMAIN_ESCAPE
+    while the requests beside it complete normally and equal their run alone;
+    an empty request (a box, no particles) completes with no particles; zero
+    steps is an argument error."""
+    good = req_scene(80, 5000)
+    srv = bm.Server()
+    rid = srv.submit(good, 40)
+    assert srv.wait(rid) == 0
+    alone = srv.result(rid)
+    srv.close()
+
+    bad = req_scene(81, 2000)
+    bad.domain = ((8, 0, 8), (4, 4, 4))  # far too small: the sand leaves it
+    empty = dataclasses.replace(req_scene(82, 2000), position=np.zeros((0, 3), np.float32),
+                                mass=np.zeros(0, np.float32), domain=((0, 0, 0), (32, 32, 32)), bodies=[])
+    srv = bm.Server()
+    ids = [srv.submit(bad, 30), srv.submit(good, 40), srv.submit(empty, 10)]
+    assert [srv.wait(r) for r in ids] == [4, 0, 0]  # BM_ERR_DOMAIN_ESCAPE for the escaping request only
+    mixed = srv.result(ids[1])
+    e = max_err_dx(alone["position"], mixed["position"], good.dx)
+    print(f"beside a failing request: {e:.2e} dx from the run alone")
+    assert e < POS_TOL_100
+    np.testing.assert_allclose(alone["body"].center[:], mixed["body"].center[:], atol=1e-5)
+    assert srv.result(ids[2])["position"].shape == (0, 3)
+    with pytest.raises(bm.BMError):
+        srv.submit(good, 0)
+    st = srv.stats()
+    assert st["completed"] == 3
     srv.close()
 
 
