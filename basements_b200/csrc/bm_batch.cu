@@ -397,23 +397,9 @@ BM_API bm_status_t bm_batch_get_particles(bm_batch_t* b, int32_t scene, const bm
     if (!b || !v) return invalid_arg("NULL argument");
     if (scene < 0 || scene >= (int32_t)b->w.scenes.size()) return BM_ERR_NOT_FOUND;
     DeviceGuard dg(b->w.device);
-    SceneHost& h = b->w.scenes[scene];
-    const int64_t n = h.n();
-    if (n == 0) return BM_OK;
-    const ParticleSoA& ps = h.dev.store[b->w.sel];
-    struct Field { float* dst; int plane; int width; };
-    const Field fields[] = {{v->position, P_X, 3}, {v->velocity, P_V, 3}, {v->F, P_F, 9},
-                            {v->C, P_C, 9},        {v->mass, P_M, 1},     {v->volume, P_V0, 1}};
-    float* tmp = nullptr;
-    BM_CHECK_CUDA(cudaMallocAsync((void**)&tmp, sizeof(float) * 9 * n, b->w.stream));
-    for (const Field& f : fields) {
-        if (!f.dst) continue;
-        launch_gather_rows(ps, f.plane, f.width, tmp, b->w.stream);
-        cudaMemcpyAsync(f.dst, tmp, sizeof(float) * f.width * n, cudaMemcpyDeviceToHost, b->w.stream);
-    }
-    cudaFreeAsync(tmp, b->w.stream);
-    BM_CHECK_CUDA(cudaStreamSynchronize(b->w.stream));
-    return launch_status("batch_get_particles");
+    const World::ReadField fields[] = {{v->position, P_X, 3}, {v->velocity, P_V, 3}, {v->F, P_F, 9},
+                                       {v->C, P_C, 9},        {v->mass, P_M, 1},     {v->volume, P_V0, 1}};
+    return b->w.read_fields(b->w.scenes[scene], fields, 6);
 }
 
 BM_API bm_status_t bm_batch_get_body(bm_batch_t* b, int32_t scene, bm_collider_t* out) {

@@ -425,26 +425,9 @@ BM_API bm_status_t bm_solver_num_particles(bm_solver_t* s, int64_t* out) {
 BM_API bm_status_t bm_solver_get_particles(bm_solver_t* s, const bm_particles_view_t* v) {
     if (!s || !v) return invalid_arg("NULL argument");
     DeviceGuard dg(s->w.device);
-    const int64_t n = s->sc().n();
-    if (n == 0) return BM_OK;
-    const ParticleSoA& ps = s->sc().dev.store[s->w.sel];
-    struct Field { float* dst; int plane; int width; };
-    const Field fields[] = {{v->position, P_X, 3}, {v->velocity, P_V, 3}, {v->F, P_F, 9},
-                            {v->C, P_C, 9},        {v->mass, P_M, 1},     {v->volume, P_V0, 1}};
-    float* tmp = nullptr;
-    BM_CHECK_CUDA(cudaMallocAsync((void**)&tmp, sizeof(float) * 9 * n, s->w.stream));
-    bm_status_t st = BM_OK;
-    for (const Field& f : fields) {
-        if (!f.dst) continue;
-        launch_gather_rows(ps, f.plane, f.width, tmp, s->w.stream);
-        if (cudaMemcpyAsync(f.dst, tmp, sizeof(float) * f.width * n, cudaMemcpyDeviceToHost, s->w.stream) !=
-            cudaSuccess)
-            st = BM_ERR_CUDA;
-    }
-    cudaFreeAsync(tmp, s->w.stream);
-    BM_CHECK_CUDA(cudaStreamSynchronize(s->w.stream));
-    if (st != BM_OK) set_last_error("device-to-host copy of particles failed");
-    return st;
+    const World::ReadField fields[] = {{v->position, P_X, 3}, {v->velocity, P_V, 3}, {v->F, P_F, 9},
+                                       {v->C, P_C, 9},        {v->mass, P_M, 1},     {v->volume, P_V0, 1}};
+    return s->w.read_fields(s->sc(), fields, 6);
 }
 
 BM_API bm_status_t bm_solver_set_particles(bm_solver_t* s, int64_t first, int64_t n, const bm_particles_view_t* v) {

@@ -1,12 +1,64 @@
 // bm_world.cu — host core shared by the plain solver, the batch and the server.
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
-
 #include <cstring>
+#include <mutex>
+#include <system_error>
+#include <thread>
+#include <vector>
 
 #include "bm_world.h"
 
 namespace bm {
+
+namespace {
+
+// Bytes per pinned read-back chunk.
+constexpr size_t kReadChunk = size_t(8) << 20;
+
+// The pinned chunk pair of read_fields, shared by every World of the process
+// and kept until it exits: pinning 16 MB takes milliseconds, more than a
+// read of millions of particles, and a solver is often created for one job.
+// Pinned memory serves every device of the process; readers take turns.
+struct ReadBack {
+    std::mutex mu;
+    void* buf[2] = {nullptr, nullptr};
+};
+
+ReadBack& read_back() {
+    static ReadBack* r = new ReadBack;  // never destroyed: no teardown-order question
+    return *r;
+}
+
+// memcpy into pageable memory. A fresh destination (a new numpy array) takes
+// a page fault per page on first touch, and those dominate the copy, so parts
+// of at least 2 MB go to up to four threads.
+void copy_out(void* dst, const void* src, size_t bytes) {
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(4, hw), std::max<size_t>(1, bytes >> 21));
+    const size_t part = (bytes / nt + 63) & ~size_t(63);
+    // piece t is [part t, part (t+1)), the last one ending at `bytes`
+    auto piece = [=](size_t t) {
+        const size_t o = std::min(bytes, part * t);
+        const size_t e = t + 1 == nt ? bytes : std::min(bytes, part * (t + 1));
+        if (e > o) std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, e - o);
+    };
+    std::vector<std::thread> threads;
+    size_t t = 1;
+    for (; t < nt; ++t) {
+        try {
+            threads.emplace_back(piece, t);
+        } catch (const std::system_error&) {
+            break;
+        }
+    }
+    for (size_t r = t; r < nt; ++r) piece(r);  // the pieces no thread took
+    piece(0);
+    for (auto& th : threads) th.join();
+}
+
+}  // namespace
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& s) { g_last_error = s; }
@@ -169,6 +221,8 @@ void World::release() {
         stage_cap[k] = 0;
         if (stage_used[k]) cudaEventDestroy(stage_used[k]);
         stage_used[k] = nullptr;
+        if (read_done[k]) cudaEventDestroy(read_done[k]);
+        read_done[k] = nullptr;
     }
     if (upload_done) cudaEventDestroy(upload_done);
     upload_done = nullptr;
@@ -252,13 +306,68 @@ bm_status_t World::ensure_particle_capacity(SceneHost& h, int64_t need) {
 }
 
 void World::update_bbox(SceneHost& h, int64_t n, const float* pos) {
+    if (h.domain_set || h.grid_ready) return;  // the box is fixed: the bounds are never read
+    // finite coordinates only; min/max in float convert exactly to double
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    bool any[3] = {false, false, false};
     for (int64_t p = 0; p < n; ++p)
         for (int a = 0; a < 3; ++a) {
-            const double v = pos[3 * p + a];
-            if (!std::isfinite(v)) continue;
-            h.bbox_lo[a] = std::min(h.bbox_lo[a], v);
-            h.bbox_hi[a] = std::max(h.bbox_hi[a], v);
+            const float v = pos[3 * p + a];
+            const bool ok = std::fabs(v) <= FLT_MAX;  // false for NaN and infinities
+            lo[a] = ok && v < lo[a] ? v : lo[a];
+            hi[a] = ok && v > hi[a] ? v : hi[a];
+            any[a] = any[a] || ok;
         }
+    for (int a = 0; a < 3; ++a)
+        if (any[a]) {
+            h.bbox_lo[a] = std::min(h.bbox_lo[a], (double)lo[a]);
+            h.bbox_hi[a] = std::max(h.bbox_hi[a], (double)hi[a]);
+        }
+}
+
+bm_status_t World::read_fields(SceneHost& h, const ReadField* fields, int n_fields) {
+    const int64_t n = h.n();
+    if (n == 0) return BM_OK;
+    const ParticleSoA& ps = h.dev.store[sel];
+    // the sort's destination store is scratch between steps (N_PLANES >= 9
+    // floats per particle)
+    float* rows = h.dev.store[sel ^ 1].base;
+    ReadBack& rb = read_back();
+    std::lock_guard<std::mutex> lk(rb.mu);
+    void* const* read_buf = rb.buf;
+    for (int k = 0; k < 2; ++k) {
+        if (!rb.buf[k]) BM_CHECK_CUDA(cudaMallocHost(&rb.buf[k], kReadChunk));
+        if (!read_done[k]) BM_CHECK_CUDA(cudaEventCreateWithFlags(&read_done[k], cudaEventDisableTiming));
+    }
+    for (int f = 0; f < n_fields; ++f) {
+        if (!fields[f].dst) continue;
+        launch_gather_rows(ps, fields[f].plane, fields[f].width, rows, stream);
+        char* dst = reinterpret_cast<char*>(fields[f].dst);
+        const char* src = reinterpret_cast<const char*>(rows);
+        const size_t bytes = sizeof(float) * (size_t)fields[f].width * (size_t)n;
+        // the DMA of chunk i overlaps the host copy of chunk i-1 (a buffer is
+        // refilled only after its host copy returned)
+        size_t off = 0, prev_off = 0, prev_len = 0;
+        int k = 0;
+        while (off < bytes) {
+            const size_t len = std::min(kReadChunk, bytes - off);
+            BM_CHECK_CUDA(cudaMemcpyAsync(read_buf[k], src + off, len, cudaMemcpyDeviceToHost, stream));
+            BM_CHECK_CUDA(cudaEventRecord(read_done[k], stream));
+            if (prev_len) {
+                BM_CHECK_CUDA(cudaEventSynchronize(read_done[k ^ 1]));
+                copy_out(dst + prev_off, read_buf[k ^ 1], prev_len);
+            }
+            prev_off = off;
+            prev_len = len;
+            k ^= 1;
+            off += len;
+        }
+        if (prev_len) {
+            BM_CHECK_CUDA(cudaEventSynchronize(read_done[k ^ 1]));
+            copy_out(dst + prev_off, read_buf[k ^ 1], prev_len);
+        }
+    }
+    return launch_status("read particles");
 }
 
 bm_status_t World::append_particles(SceneHost& h, int64_t n, const float* pos, const float* vel, const float* mass) {

@@ -66,6 +66,9 @@ public:
     size_t stage_cap[2] = {0, 0};
     cudaEvent_t stage_used[2] = {nullptr, nullptr};
     int stage_next = 0;
+    // Events of the pinned chunk pair through which read_fields brings
+    // particle rows back into pageable host arrays.
+    cudaEvent_t read_done[2] = {nullptr, nullptr};
     std::vector<SceneHost> scenes;
     int cur = 0;  // accumulation buffer of the current step
     int sel = 0;  // current particle store
@@ -98,6 +101,11 @@ public:
     bm_status_t ensure_grid(SceneHost& h);
     bm_status_t append_particles(SceneHost& h, int64_t n, const float* pos, const float* vel, const float* mass);
     void update_bbox(SceneHost& h, int64_t n, const float* pos);
+    // Copies fields of a scene's particles (AoS rows, add order) into host
+    // arrays: rows gathered into the idle particle store, brought back
+    // through the pinned chunk pair. Waits for the copies.
+    struct ReadField { float* dst; int plane; int width; };
+    bm_status_t read_fields(SceneHost& h, const ReadField* fields, int n_fields);
     void free_scene(SceneHost& h);
     void remove_scene(int index);
     // P2G into acc[cur] of the scenes flagged `fresh` (their accumulators
