@@ -17,10 +17,11 @@ namespace {
 // Bytes per pinned read-back chunk.
 constexpr size_t kReadChunk = size_t(8) << 20;
 
-// The pinned chunk pair of read_fields, shared by every World of the process
-// and kept until it exits: pinning 16 MB takes milliseconds, more than a
-// read of millions of particles, and a solver is often created for one job.
-// Pinned memory serves every device of the process; readers take turns.
+// The pinned chunk pair of read_fields and upload_bytes, shared by every
+// World of the process and kept until it exits: pinning 16 MB takes
+// milliseconds, more than a read of millions of particles, and a solver is
+// often created for one job. Pinned memory serves every device of the
+// process; callers take turns.
 struct ReadBack {
     std::mutex mu;
     void* buf[2] = {nullptr, nullptr};
@@ -31,10 +32,10 @@ ReadBack& read_back() {
     return *r;
 }
 
-// memcpy into pageable memory. A fresh destination (a new numpy array) takes
-// a page fault per page on first touch, and those dominate the copy, so parts
-// of at least 2 MB go to up to four threads.
-void copy_out(void* dst, const void* src, size_t bytes) {
+// memcpy between pinned and pageable memory, in parts of at least 2 MB on up
+// to four threads. A fresh pageable destination (a new numpy array) takes a
+// page fault per page on first touch, and those dominate such a copy.
+void host_copy(void* dst, const void* src, size_t bytes) {
     const size_t hw = std::max(1u, std::thread::hardware_concurrency());
     const size_t nt = std::min<size_t>(std::min<size_t>(4, hw), std::max<size_t>(1, bytes >> 21));
     const size_t part = (bytes / nt + 63) & ~size_t(63);
@@ -325,6 +326,36 @@ void World::update_bbox(SceneHost& h, int64_t n, const float* pos) {
         }
 }
 
+bm_status_t World::upload_bytes(void* d_dst, const void* h_src, size_t bytes) {
+    ReadBack& rb = read_back();
+    std::lock_guard<std::mutex> lk(rb.mu);
+    for (int k = 0; k < 2; ++k) {
+        if (!rb.buf[k]) BM_CHECK_CUDA(cudaMallocHost(&rb.buf[k], kReadChunk));
+        if (!read_done[k]) BM_CHECK_CUDA(cudaEventCreateWithFlags(&read_done[k], cudaEventDisableTiming));
+    }
+    const char* src = static_cast<const char*>(h_src);
+    char* dst = static_cast<char*>(d_dst);
+    // chunk i is copied into a pinned buffer while the DMA of chunk i-1 runs;
+    // a buffer is refilled only after the DMA that read it finished
+    bool in_flight[2] = {false, false};
+    size_t off = 0;
+    int k = 0;
+    while (off < bytes) {
+        const size_t len = std::min(kReadChunk, bytes - off);
+        if (in_flight[k]) BM_CHECK_CUDA(cudaEventSynchronize(read_done[k]));
+        host_copy(rb.buf[k], src + off, len);
+        BM_CHECK_CUDA(cudaMemcpyAsync(dst + off, rb.buf[k], len, cudaMemcpyHostToDevice, upload));
+        BM_CHECK_CUDA(cudaEventRecord(read_done[k], upload));
+        in_flight[k] = true;
+        k ^= 1;
+        off += len;
+    }
+    // the pinned pair is shared: its DMAs end before another caller may refill it
+    for (int q = 0; q < 2; ++q)
+        if (in_flight[q]) BM_CHECK_CUDA(cudaEventSynchronize(read_done[q]));
+    return BM_OK;
+}
+
 bm_status_t World::read_fields(SceneHost& h, const ReadField* fields, int n_fields) {
     const int64_t n = h.n();
     if (n == 0) return BM_OK;
@@ -355,7 +386,7 @@ bm_status_t World::read_fields(SceneHost& h, const ReadField* fields, int n_fiel
             BM_CHECK_CUDA(cudaEventRecord(read_done[k], stream));
             if (prev_len) {
                 BM_CHECK_CUDA(cudaEventSynchronize(read_done[k ^ 1]));
-                copy_out(dst + prev_off, read_buf[k ^ 1], prev_len);
+                host_copy(dst + prev_off, read_buf[k ^ 1], prev_len);
             }
             prev_off = off;
             prev_len = len;
@@ -364,7 +395,7 @@ bm_status_t World::read_fields(SceneHost& h, const ReadField* fields, int n_fiel
         }
         if (prev_len) {
             BM_CHECK_CUDA(cudaEventSynchronize(read_done[k ^ 1]));
-            copy_out(dst + prev_off, read_buf[k ^ 1], prev_len);
+            host_copy(dst + prev_off, read_buf[k ^ 1], prev_len);
         }
     }
     return launch_status("read particles");
@@ -383,9 +414,10 @@ bm_status_t World::append_particles(SceneHost& h, int64_t n, const float* pos, c
     float* d_pos = rows;
     float* d_mass = rows + 3 * (size_t)n;
     float* d_vel = vel ? rows + 4 * (size_t)n : nullptr;
-    BM_CHECK_CUDA(cudaMemcpyAsync(d_pos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, upload));
-    if (mass) BM_CHECK_CUDA(cudaMemcpyAsync(d_mass, mass, sizeof(float) * n, cudaMemcpyHostToDevice, upload));
-    if (vel) BM_CHECK_CUDA(cudaMemcpyAsync(d_vel, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, upload));
+    st = upload_bytes(d_pos, pos, sizeof(float) * 3 * n);
+    if (st == BM_OK && mass) st = upload_bytes(d_mass, mass, sizeof(float) * n);
+    if (st == BM_OK && vel) st = upload_bytes(d_vel, vel, sizeof(float) * 3 * n);
+    if (st != BM_OK) return st;
     BM_CHECK_CUDA(cudaEventRecord(upload_done, upload));
     BM_CHECK_CUDA(cudaStreamWaitEvent(stream, upload_done, 0));
     launch_fill_particles(h.dev.store[sel], n0, n, d_pos, d_vel, mass ? d_mass : nullptr, h.density, stream);

@@ -67,7 +67,8 @@ public:
     cudaEvent_t stage_used[2] = {nullptr, nullptr};
     int stage_next = 0;
     // Events of the pinned chunk pair through which read_fields brings
-    // particle rows back into pageable host arrays.
+    // particle rows back into pageable host arrays and upload_bytes sends
+    // them up.
     cudaEvent_t read_done[2] = {nullptr, nullptr};
     std::vector<SceneHost> scenes;
     int cur = 0;  // accumulation buffer of the current step
@@ -106,6 +107,9 @@ public:
     // through the pinned chunk pair. Waits for the copies.
     struct ReadField { float* dst; int plane; int width; };
     bm_status_t read_fields(SceneHost& h, const ReadField* fields, int n_fields);
+    // Host-to-device copy on the upload stream through the same pinned pair;
+    // returns when the copy has landed.
+    bm_status_t upload_bytes(void* d_dst, const void* h_src, size_t bytes);
     void free_scene(SceneHost& h);
     void remove_scene(int index);
     // P2G into acc[cur] of the scenes flagged `fresh` (their accumulators
