@@ -6,6 +6,7 @@
 #include <mutex>
 #include <system_error>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "bm_world.h"
@@ -30,6 +31,50 @@ struct ReadBack {
 ReadBack& read_back() {
     static ReadBack* r = new ReadBack;  // never destroyed: no teardown-order question
     return *r;
+}
+
+// Pinned staging blocks of released Worlds, handed to the next World of the
+// process: pinning host memory costs about a millisecond per call, as much as
+// a short job's table uploads. At most kKeptStageBlocks are kept.
+constexpr size_t kKeptStageBlocks = 16;
+
+struct StagePool {
+    std::mutex mu;
+    std::vector<std::pair<size_t, void*>> blocks;  // (capacity, pointer)
+};
+
+StagePool& stage_pool() {
+    static StagePool* p = new StagePool;  // never destroyed: no teardown-order question
+    return *p;
+}
+
+// A kept block of at least `bytes` (the smallest such), or none.
+bool take_stage_block(size_t bytes, void** buf, size_t* cap) {
+    StagePool& sp = stage_pool();
+    std::lock_guard<std::mutex> lk(sp.mu);
+    int best = -1;
+    for (int i = 0; i < (int)sp.blocks.size(); ++i)
+        if (sp.blocks[i].first >= bytes && (best < 0 || sp.blocks[i].first < sp.blocks[best].first)) best = i;
+    if (best < 0) return false;
+    *cap = sp.blocks[best].first;
+    *buf = sp.blocks[best].second;
+    sp.blocks.erase(sp.blocks.begin() + best);
+    return true;
+}
+
+// Keeps a block for a later World, or unpins it when enough are kept. The
+// caller guarantees that no copy still reads it.
+void give_stage_block(void* buf, size_t cap) {
+    if (!buf) return;
+    StagePool& sp = stage_pool();
+    {
+        std::lock_guard<std::mutex> lk(sp.mu);
+        if (sp.blocks.size() < kKeptStageBlocks) {
+            sp.blocks.emplace_back(cap, buf);
+            return;
+        }
+    }
+    cudaFreeHost(buf);
 }
 
 // memcpy between pinned and pageable memory, in parts of at least 2 MB on up
@@ -140,12 +185,14 @@ bm_status_t World::stage_begin(size_t bytes, void** out) {
     const int k = stage_next;
     BM_CHECK_CUDA(cudaEventSynchronize(stage_used[k]));  // the copies that last read this buffer ran
     if (stage_cap[k] < bytes) {
-        cudaFreeHost(stage_buf[k]);
+        give_stage_block(stage_buf[k], stage_cap[k]);
         stage_buf[k] = nullptr;
         stage_cap[k] = 0;
-        const size_t cap = std::max<size_t>(bytes * 2, 1 << 16);
-        BM_CHECK_CUDA(cudaMallocHost(&stage_buf[k], cap));
-        stage_cap[k] = cap;
+        if (!take_stage_block(bytes, &stage_buf[k], &stage_cap[k])) {
+            const size_t cap = std::max<size_t>(bytes * 2, 1 << 16);
+            BM_CHECK_CUDA(cudaMallocHost(&stage_buf[k], cap));
+            stage_cap[k] = cap;
+        }
     }
     *out = stage_buf[k];
     return BM_OK;
@@ -217,7 +264,7 @@ void World::release() {
     if (stream) cudaStreamSynchronize(stream);
     if (upload) cudaStreamSynchronize(upload);
     for (int k = 0; k < 2; ++k) {
-        cudaFreeHost(stage_buf[k]);
+        give_stage_block(stage_buf[k], stage_cap[k]);  // the streams are idle: no copy reads it
         stage_buf[k] = nullptr;
         stage_cap[k] = 0;
         if (stage_used[k]) cudaEventDestroy(stage_used[k]);
