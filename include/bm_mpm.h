@@ -139,11 +139,15 @@ BM_API bm_status_t bm_solver_set_gravity(bm_solver_t* s, const float gravity[3])
 BM_API bm_status_t bm_solver_set_plastic_alpha(bm_solver_t* s, float alpha);           /* :53 */
 BM_API bm_status_t bm_solver_set_floor_friction(bm_solver_t* s, float mu_floor);       /* :54 */
 /* add_particle (:23-34) for n particles: V0 = m / rho, F = I, C = 0.
- * velocity NULL means zero, mass NULL means 1.0 (the reference default). */
+ * velocity NULL means zero, mass NULL means 1.0 (the reference default).
+ * Returns when the arrays have been copied (through the process's pinned
+ * chunk pair): the caller may reuse them at once. */
 BM_API bm_status_t bm_solver_add_particles(bm_solver_t* s, int64_t n, const float* position,
                                            const float* velocity, const float* mass);
 BM_API bm_status_t bm_solver_num_particles(bm_solver_t* s, int64_t* out);
-/* get_particles (:89): device-to-host copy into the caller's SoA view. */
+/* get_particles (:89): device-to-host copy into the caller's SoA view
+ * (rows of each field, add order), through the process's pinned chunk pair;
+ * returns when the copies have landed. */
 BM_API bm_status_t bm_solver_get_particles(bm_solver_t* s, const bm_particles_view_t* view);
 /* get_particles_mutable (:59): overwrite fields of particles [first, first+n);
  * NULL fields are left as they are. mass/volume are ignored. */
