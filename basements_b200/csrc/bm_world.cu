@@ -33,6 +33,19 @@ ReadBack& read_back() {
     return *r;
 }
 
+// Waits, on every exit of a holder of the ReadBack lock, for the copies that
+// still use the pinned pair (error paths included), so that the next holder
+// never refills a buffer a copy is reading or writing. Declared after the
+// lock, it runs before the unlock.
+struct DrainPinned {
+    cudaEvent_t* done;
+    bool in_flight[2] = {false, false};
+    ~DrainPinned() {
+        for (int q = 0; q < 2; ++q)
+            if (in_flight[q]) cudaEventSynchronize(done[q]);
+    }
+};
+
 // Pinned staging blocks of released Worlds, handed to the next World of the
 // process: pinning host memory costs about a millisecond per call, as much as
 // a short job's table uploads. At most kKeptStageBlocks are kept.
@@ -380,26 +393,26 @@ bm_status_t World::upload_bytes(void* d_dst, const void* h_src, size_t bytes) {
         if (!rb.buf[k]) BM_CHECK_CUDA(cudaMallocHost(&rb.buf[k], kReadChunk));
         if (!read_done[k]) BM_CHECK_CUDA(cudaEventCreateWithFlags(&read_done[k], cudaEventDisableTiming));
     }
+    DrainPinned drain{read_done};
     const char* src = static_cast<const char*>(h_src);
     char* dst = static_cast<char*>(d_dst);
     // chunk i is copied into a pinned buffer while the DMA of chunk i-1 runs;
     // a buffer is refilled only after the DMA that read it finished
-    bool in_flight[2] = {false, false};
     size_t off = 0;
     int k = 0;
     while (off < bytes) {
         const size_t len = std::min(kReadChunk, bytes - off);
-        if (in_flight[k]) BM_CHECK_CUDA(cudaEventSynchronize(read_done[k]));
+        if (drain.in_flight[k]) BM_CHECK_CUDA(cudaEventSynchronize(read_done[k]));
         host_copy(rb.buf[k], src + off, len);
+        drain.in_flight[k] = true;  // from here a failed enqueue may still have left a copy running
         BM_CHECK_CUDA(cudaMemcpyAsync(dst + off, rb.buf[k], len, cudaMemcpyHostToDevice, upload));
         BM_CHECK_CUDA(cudaEventRecord(read_done[k], upload));
-        in_flight[k] = true;
         k ^= 1;
         off += len;
     }
     // the pinned pair is shared: its DMAs end before another caller may refill it
     for (int q = 0; q < 2; ++q)
-        if (in_flight[q]) BM_CHECK_CUDA(cudaEventSynchronize(read_done[q]));
+        if (drain.in_flight[q]) BM_CHECK_CUDA(cudaEventSynchronize(read_done[q]));
     return BM_OK;
 }
 
@@ -417,6 +430,7 @@ bm_status_t World::read_fields(SceneHost& h, const ReadField* fields, int n_fiel
         if (!rb.buf[k]) BM_CHECK_CUDA(cudaMallocHost(&rb.buf[k], kReadChunk));
         if (!read_done[k]) BM_CHECK_CUDA(cudaEventCreateWithFlags(&read_done[k], cudaEventDisableTiming));
     }
+    DrainPinned drain{read_done};
     for (int f = 0; f < n_fields; ++f) {
         if (!fields[f].dst) continue;
         launch_gather_rows(ps, fields[f].plane, fields[f].width, rows, stream);
@@ -429,6 +443,7 @@ bm_status_t World::read_fields(SceneHost& h, const ReadField* fields, int n_fiel
         int k = 0;
         while (off < bytes) {
             const size_t len = std::min(kReadChunk, bytes - off);
+            drain.in_flight[k] = true;
             BM_CHECK_CUDA(cudaMemcpyAsync(read_buf[k], src + off, len, cudaMemcpyDeviceToHost, stream));
             BM_CHECK_CUDA(cudaEventRecord(read_done[k], stream));
             if (prev_len) {
