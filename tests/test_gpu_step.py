@@ -302,3 +302,43 @@ def test_get_and_set_particles_keep_add_order():
     s.step(sc.dt, 10)
     r.step(sc.dt, 10)
     assert max_err_dx(s.get_particles()["position"], r.get_particles()["position"], sc.dx) < POS_TOL_100
+
+
+def test_wheel_rut_full_size_matches_reference_for_three_coupled_steps():
+    """The benchmark's own workload at full size: 2M particles in the 128^3
+    box with the M1 cylinder rolling through them. Three coupled steps
+    against the reference on the CPU (about 7 s on one core): positions,
+    velocities and the reaction of every step; afterwards grid mass equals
+    particle mass, and no particle escaped, turned non-finite or left a
+    light-node suspect."""
+    sc = scenes.wheel_rut(n_keep=2_000_000)
+    body = sc.bodies[0]
+    g = bm.MPMSolver(sc.dx, domain=sc.domain)
+    g.set_material(sc.E, sc.nu, sc.rho)
+    g.set_plastic_alpha(sc.alpha)
+    g.add_particles(sc.position, None, sc.mass)
+    c = O.CpuSolver(REF, sc.dx)
+    c.set_material(sc.E, sc.nu, sc.rho)
+    c.set_plastic_alpha(sc.alpha)
+    c.add_particles(sc.position, None, sc.mass)
+    for i in range(3):
+        col = body.at_time(i * sc.dt).as_tuple()
+        f, t, n_in = g.step_coupled(sc.dt, [bm.make_collider(**col)])[0]
+        c.p2g(sc.dt)
+        c.grid_update(sc.dt)
+        rf, rt, rn = c.m1_apply(O.collider(**col), sc.dt)
+        c.g2p(sc.dt)
+        print(f"step {i}: force {f} vs {rf}, nodes inside {n_in} vs {rn}")
+        assert n_in > 0 and abs(n_in - rn) <= 2
+        np.testing.assert_allclose(f, rf, rtol=1e-4, atol=1e-4 * np.abs(rf).max())
+        np.testing.assert_allclose(t, rt, rtol=1e-4, atol=1e-4 * max(np.abs(rt).max(), 1e-3 * np.abs(rf).max()))
+    pg, pc = g.get_particles(("position", "velocity")), c.get_particles()
+    e = max_err_dx(pg["position"], pc["position"], sc.dx)
+    print(f"wheel rut 2M, 3 steps: max |x_gpu - x_ref| = {e:.2e} dx")
+    assert e < 1e-5
+    np.testing.assert_allclose(pg["velocity"], pc["velocity"], atol=1e-5)
+    assert g.sync() == (0, 0) and g.light_node_suspects() == 0
+    g.p2g(sc.dt)
+    grid_mass = g.get_grid()["mass"].astype(np.float64).sum()
+    pm = sc.mass.astype(np.float64).sum()
+    assert abs(grid_mass - pm) / pm < MASS_REL_TOL
