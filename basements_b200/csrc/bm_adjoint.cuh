@@ -16,10 +16,11 @@
 // adjoint therefore differentiates the algorithm itself: the rotations are
 // replayed with the same thresholds and the reverse pass goes back through
 // them one by one (between two decisions the computed function is smooth and
-// this is its exact derivative). The replay and the reverse pass run in
-// double: their terms scale with 1/a_ij and cancel, and in float the result
-// loses percents at small strains. They follow the algorithm as the FP64 path
-// runs it, at the state the FP32 forward produced.
+// this is its exact derivative). The forward records each rotation and the
+// reverse pass undoes them in turn. Both run in double: their terms scale
+// with 1/a_ij and cancel, and in float the result loses percents at small
+// strains. They follow the algorithm as the FP64 path runs it, at the state
+// the FP32 forward produced.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -33,11 +34,13 @@ namespace adj {
 template <int a, int b> __device__ __forceinline__ constexpr int uix() { return a < b ? 3 * a + b : 3 * b + a; }
 
 // One Jacobi rotation of svd3 (bm_math.cuh, jacobi_rotate) in double.
+// Returns whether it rotated, and then its (c, s).
 template <int I, int J, int K>
-__device__ __forceinline__ void jacobi_rotate_d(double A[9], double V[9], double& max_off) {
+__device__ __forceinline__ bool jacobi_rotate_d(double A[9], double V[9], double& max_off, double& c_out,
+                                                double& s_out) {
     const double a_ij = A[3 * I + J], a_ii = A[3 * I + I], a_jj = A[3 * J + J];
     max_off = fmax(max_off, fabs(a_ij));
-    if (fabs(a_ij) < 1e-6) return;
+    if (fabs(a_ij) < 1e-6) return false;
     const double tau = (a_jj - a_ii) / (2.0 * a_ij);
     const double t = tau >= 0.0 ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
     const double c = 1.0 / sqrt(1.0 + t * t);
@@ -60,34 +63,36 @@ __device__ __forceinline__ void jacobi_rotate_d(double A[9], double V[9], double
         const double vri = V[3 * r + I], vrj = V[3 * r + J];
         V[3 * r + I] = c * vri - s * vrj;
         V[3 * r + J] = s * vri + c * vrj;
-    }
+    }    c_out = c;
+    s_out = s;
+    return true;
 }
 
-// A = F^T F, V = I and the sweeps, stopped before rotation slot `upto`
-// (slot q = 3 * sweep + pair). Returns the number of slots reached.
-__device__ __forceinline__ int jacobi_replay(const double F[9], int upto, double A[9], double V[9]) {
+// Undoes a rotation of jacobi_rotate_d from its (c, s). The rotation is the
+// similarity A' = G^T A G, V' = V G with G = [[c, s], [-s, c]] in the (I, J)
+// plane, so A = G A' G^T and V = V' G^T (one rounding in double; the
+// rotation's own zero of a'_ij is what that similarity gives up to rounding).
+template <int I, int J, int K>
+__device__ __forceinline__ void jacobi_unrotate_d(double A[9], double V[9], double c, double s) {
+    const double a_ii = A[3 * I + I], a_jj = A[3 * J + J], a_ij = A[3 * I + J];
+    const double cc = c * c, ss = s * s, cs = c * s;
+    const double o_ij = cs * (a_jj - a_ii) + (cc - ss) * a_ij;
+    A[3 * I + I] = cc * a_ii + 2.0 * cs * a_ij + ss * a_jj;
+    A[3 * J + J] = ss * a_ii - 2.0 * cs * a_ij + cc * a_jj;
+    A[3 * I + J] = o_ij;
+    A[3 * J + I] = o_ij;
+    const double nik = A[3 * I + K], njk = A[3 * J + K];
+    const double aik = c * nik + s * njk, ajk = -s * nik + c * njk;
+    A[3 * I + K] = aik;
+    A[3 * K + I] = aik;
+    A[3 * J + K] = ajk;
+    A[3 * K + J] = ajk;
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) A[3 * i + j] = (F[i] * F[j] + F[3 + i] * F[3 + j]) + F[6 + i] * F[6 + j];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) V[q] = (q % 4 == 0) ? 1.0 : 0.0;
-    int q = 0;
-#pragma unroll 1
-    for (int sweep = 0; sweep < 5; ++sweep) {
-        double max_off = 0.0;
-        if (q == upto) return q;
-        jacobi_rotate_d<0, 1, 2>(A, V, max_off);
-        ++q;
-        if (q == upto) return q;
-        jacobi_rotate_d<0, 2, 1>(A, V, max_off);
-        ++q;
-        if (q == upto) return q;
-        jacobi_rotate_d<1, 2, 0>(A, V, max_off);
-        ++q;
-        if (max_off < 1e-5) break;
+    for (int r = 0; r < 3; ++r) {
+        const double vi = V[3 * r + I], vj = V[3 * r + J];
+        V[3 * r + I] = c * vi + s * vj;
+        V[3 * r + J] = -s * vi + c * vj;
     }
-    return q;
 }
 
 // Reverse of one jacobi_rotate_d<I,J,K> applied to (A, V) (the state before
@@ -133,14 +138,41 @@ __device__ __forceinline__ void jacobi_rotate_adjoint(const double A[9], const d
     Ab[uix<I, J>()] -= taub * tau / a_ij;
 }
 
-// The SVD forward with what its adjoint needs.
+// The SVD forward with what its adjoint needs: the final A and V, and the
+// rotation of every slot (slot q = 3 * sweep + pair), so that the reverse
+// pass undoes the rotations one by one instead of replaying the sweeps.
 struct SvdD {
     double A[9], V[9], U[9], S[3];
-    int n;  // rotation slots reached
+    double c[15], s[15];  // (c, s) of slot q when it rotated
+    unsigned applied;     // bit q: slot q rotated (else it was skipped, the identity)
+    int n;                // rotation slots reached
 };
 
+// A = F^T F, V = I and the sweeps of svd3 (at most 5, a pair skipped below
+// 1e-6, stopped when the sweep's largest off-diagonal is below 1e-5).
 __device__ __forceinline__ void svd_forward(const double F[9], SvdD& f) {
-    f.n = jacobi_replay(F, 1 << 20, f.A, f.V);
+    double* A = f.A;
+    double* V = f.V;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) A[3 * i + j] = (F[i] * F[j] + F[3 + i] * F[3 + j]) + F[6 + i] * F[6 + j];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) V[q] = (q % 4 == 0) ? 1.0 : 0.0;
+    f.applied = 0u;
+    int q = 0;
+#pragma unroll 1
+    for (int sweep = 0; sweep < 5; ++sweep) {
+        double max_off = 0.0;
+        if (jacobi_rotate_d<0, 1, 2>(A, V, max_off, f.c[q], f.s[q])) f.applied |= 1u << q;
+        ++q;
+        if (jacobi_rotate_d<0, 2, 1>(A, V, max_off, f.c[q], f.s[q])) f.applied |= 1u << q;
+        ++q;
+        if (jacobi_rotate_d<1, 2, 0>(A, V, max_off, f.c[q], f.s[q])) f.applied |= 1u << q;
+        ++q;
+        if (max_off < 1e-5) break;
+    }
+    f.n = q;
 #pragma unroll
     for (int k = 0; k < 3; ++k) f.S[k] = sqrt(fmax(0.0, f.A[4 * k]));
 #pragma unroll
@@ -185,15 +217,28 @@ __device__ __forceinline__ void svd_adjoint(const double F[9], const SvdD& f, co
 #pragma unroll
     for (int k = 0; k < 3; ++k)
         if (f.A[4 * k] > 0.0 && f.S[k] > 0.0) Ab[4 * k] = Sb[k] / (2.0 * f.S[k]);
-    // back through the rotations, last first
+    // back through the rotations, last first: undo slot q to get the state
+    // before it, then take its adjoint there (a skipped slot is the identity)
+    double Ap[9], Vp[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        Ap[q] = f.A[q];
+        Vp[q] = f.V[q];
+    }
 #pragma unroll 1
     for (int q = f.n - 1; q >= 0; --q) {
-        double Ap[9], Vp[9];
-        jacobi_replay(F, q, Ap, Vp);
+        if (!((f.applied >> q) & 1u)) continue;
         const int pair = q % 3;
-        if (pair == 0) jacobi_rotate_adjoint<0, 1, 2>(Ap, Vp, Ab, Vb);
-        else if (pair == 1) jacobi_rotate_adjoint<0, 2, 1>(Ap, Vp, Ab, Vb);
-        else jacobi_rotate_adjoint<1, 2, 0>(Ap, Vp, Ab, Vb);
+        if (pair == 0) {
+            jacobi_unrotate_d<0, 1, 2>(Ap, Vp, f.c[q], f.s[q]);
+            jacobi_rotate_adjoint<0, 1, 2>(Ap, Vp, Ab, Vb);
+        } else if (pair == 1) {
+            jacobi_unrotate_d<0, 2, 1>(Ap, Vp, f.c[q], f.s[q]);
+            jacobi_rotate_adjoint<0, 2, 1>(Ap, Vp, Ab, Vb);
+        } else {
+            jacobi_unrotate_d<1, 2, 0>(Ap, Vp, f.c[q], f.s[q]);
+            jacobi_rotate_adjoint<1, 2, 0>(Ap, Vp, Ab, Vb);
+        }
     }
     // A = F^T F (unique entries)
 #pragma unroll
