@@ -5,7 +5,6 @@ and the findings of scripts/reproduce_findings.py reaching the verdicts the
 reference's own outputs reach."""
 import os
 
-import numpy as np
 import pytest
 
 import basements_b200 as bm
