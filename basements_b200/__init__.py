@@ -508,6 +508,8 @@ def scene_desc(scene, keep: list) -> SceneDesc:
         d.has_body = 1
         d.body = make_collider(**b.as_tuple())
         d.body_dynamic = 0 if b.kinematic else 1
+        if b.inv_inertia is not None:
+            d.body_inv_inertia[:] = [float(v) for v in b.inv_inertia]
     return d
 
 

@@ -50,6 +50,10 @@ class Body:
     mass: float = 1.0
     shape: int = 0
     kinematic: bool = True
+    # body-space inverse inertia, row-major 3x3 (9 floats), applied to the
+    # torque as the reference's integrator does; None: the identity the
+    # reference's bodies start with
+    inv_inertia: tuple | None = None
 
     def at_time(self, t: float) -> "Body":
         """Kinematic pose after time t (constant linear velocity; the angular
@@ -99,6 +103,20 @@ def sand_column(cells=(16, 8, 16), offset=(8, 2, 8), ppc=8, grid=32, seed=0) -> 
     m = np.float32(rho * dx ** 3 / ppc)
     return Scene("sand_column", dx, grid, pos, np.full(n, m, np.float32), 3.5e5, 0.3, rho, dp_alpha(30.0),
                  1e-4, 1000)
+
+
+def pressed_box(inv_inertia=None) -> Scene:
+    """The sand column with a rotated dynamic box pressed into its top
+    surface, so that the coupler's torque spins the body from the first
+    step (the box-drop scenes fall for hundreds of steps before contact)."""
+    col = sand_column(cells=(16, 8, 16))
+    q = np.array([0.95, 0.2, 0.15, 0.18])
+    q = q / np.linalg.norm(q)
+    body = Body(center=(0.37, 0.305, 0.38), half_extents=(0.06, 0.03, 0.045), orientation=tuple(float(v) for v in q),
+                linear_velocity=(0.1, -0.4, 0.05), friction=0.5, mass=0.4, kinematic=False,
+                inv_inertia=None if inv_inertia is None else tuple(float(v) for v in np.ravel(inv_inertia)))
+    return Scene("pressed_box", col.dx, col.grid, col.position, col.mass, col.E, col.nu, col.rho, col.alpha, col.dt,
+                 col.steps, bodies=[body])
 
 
 def wheel_rut(n_keep=2_000_000, grid=128, bed_cells=(128, 40, 128), ppc=8, seed=1) -> Scene:

@@ -101,7 +101,7 @@ def load(kind: str):
         "box_drop_m1": fn("box_drop_m1", C.c_int, _f, C.c_int),
         "svd": fn("svd", None, C.c_int64, _f, _f, _f, _f),
         "run_dynamic_body": fn("run_dynamic_body", None, C.c_void_p, C.POINTER(OrcCollider), C.c_float, C.c_float,
-                               C.c_float, C.c_float, C.c_int),
+                               C.c_float, C.c_float, C.c_int, _f),
     }
     _loaded[kind] = api
     return api
@@ -250,9 +250,13 @@ class CpuSolver:
         n = self.api["m45a_apply"](self.h, C.byref(body), dt, _p(r))
         return r[:3].copy(), r[3:].copy(), int(n)
 
-    def run_dynamic_body(self, body: OrcCollider, gravity, dt, n_steps):
-        """n coupled steps with a dynamic body (updated in place and returned)."""
-        self.api["run_dynamic_body"](self.h, C.byref(body), *map(float, gravity), float(dt), int(n_steps))
+    def run_dynamic_body(self, body: OrcCollider, gravity, dt, n_steps, inv_inertia=None):
+        """n coupled steps with a dynamic body (updated in place and returned).
+        inv_inertia: body-space inverse inertia (3x3), None for the identity
+        the reference's bodies start with (rigid_body.h:121-122)."""
+        ii = None if inv_inertia is None else np.ascontiguousarray(np.asarray(inv_inertia, np.float32).reshape(9))
+        self.api["run_dynamic_body"](self.h, C.byref(body), *map(float, gravity), float(dt), int(n_steps),
+                                     None if ii is None else _p(ii))
         return body
 
     def grid_nodes(self):

@@ -79,10 +79,12 @@ ORC_EXPORT int ORC(box_drop_m1)(float* rows, int max_rows);
  * order of the research harness (bench_compare_all.cpp:96-116) around the
  * MPM phases: P2G, update_grid, weight m*g applied to the body, M1 coupler on
  * the body's current state, reaction added, TimeIntegrator step (zero
- * damping, identity body-space inverse inertia), G2P. body is updated in
- * place (center, orientation, velocities). */
+ * damping; body-space inverse inertia inv_inertia, row-major 3x3, applied to
+ * the torque as the integrator does, or the identity the reference's bodies
+ * start with when NULL), G2P. body is updated in place (center, orientation,
+ * velocities). */
 ORC_EXPORT void ORC(run_dynamic_body)(void* h, orc_collider_t* body, float gx, float gy, float gz, float dt,
-                                      int n_steps);
+                                      int n_steps, const float* inv_inertia);
 /* SVD of n row-major 3x3 matrices: U (n*9), sigma (n*3), V (n*9). */
 ORC_EXPORT void ORC(svd)(int64_t n, const float* F, float* U, float* S, float* V);
 

@@ -272,8 +272,14 @@ ORC_EXPORT int orc_box_drop_m1(float* rows, int max_rows) {
 }
 
 ORC_EXPORT void orc_run_dynamic_body(void* h, orc_collider_t* body, float gx, float gy, float gz, float dt,
-                                     int n_steps) {
+                                     int n_steps, const float* inv_inertia) {
     S* s = sv(h);
+    // integrator.h:34 applies the body-space inverse inertia to the torque as
+    // it is (rigid_body.h:121-122: the identity unless set)
+    M3<R> inv_i = M3<R>::identity();
+    if (inv_inertia)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) inv_i.m[i][j] = (R)inv_inertia[3 * i + j];
     V3<R> pos(body->center[0], body->center[1], body->center[2]);
     V3<R> vel(body->linear_velocity[0], body->linear_velocity[1], body->linear_velocity[2]);
     V3<R> omg(body->angular_velocity[0], body->angular_velocity[1], body->angular_velocity[2]);
@@ -293,7 +299,7 @@ ORC_EXPORT void orc_run_dynamic_body(void* h, orc_collider_t* body, float gx, fl
         force += r.force;
         V3<R> torque = V3<R>(0, 0, 0) + r.torque;
         vel += force * inv_mass * (R)dt;
-        omg += (M3<R>::identity() * torque) * (R)dt;
+        omg += (inv_i * torque) * (R)dt;
         pos += vel * (R)dt;
         Q4 qv{0, omg.x, omg.y, omg.z};
         Q4 dq = qmul(qv, q);

@@ -260,10 +260,14 @@ ORC_EXPORT int ref_box_drop_m1(float* rows, int max_rows) {
 }
 
 ORC_EXPORT void ref_run_dynamic_body(void* h, orc_collider_t* body, float gx, float gy, float gz, float dt,
-                                     int n_steps) {
+                                     int n_steps, const float* inv_inertia) {
     MPMSolver* s = sv(h);
     physics::RigidBody rb;
     rb.make_dynamic(body->mass);
+    if (inv_inertia)
+        rb.inv_inertia_tensor = math::Matrix3(inv_inertia[0], inv_inertia[1], inv_inertia[2], inv_inertia[3],
+                                              inv_inertia[4], inv_inertia[5], inv_inertia[6], inv_inertia[7],
+                                              inv_inertia[8]);
     rb.position = Vec3(body->center[0], body->center[1], body->center[2]);
     rb.orientation = math::Quaternion(body->orientation[0], body->orientation[1], body->orientation[2],
                                       body->orientation[3]);

@@ -383,3 +383,28 @@ def test_cpu_scene_properties(kind):
     s.add_particles(np.array([[0.5, 0.05, 0.5]], np.float32), np.array([[0, -10.0, 0]], np.float32))
     s.step(0.01, 10)
     assert s.get_particles()["position"][0, 1] >= 0.0
+
+
+def test_dynamic_body_inverse_inertia_port_vs_reference():
+    """The rigid update beside the coupler (integrator.h:19-57) with a
+    body-space inverse inertia other than the identity the reference's bodies
+    start with: the float restatement equals the compiled reference bit for
+    bit, and the tensor changes the body's spin."""
+    inv_i = np.array([[2.0, 0.3, 0.0], [0.3, 0.5, 0.1], [0.0, 0.1, 1.3]], np.float32)
+    sc = scenes.pressed_box()
+    out = {}
+    for kind in ("ref", "f32"):
+        for tag, ii in (("identity", None), ("tensor", inv_i)):
+            c = O.CpuSolver(kind, sc.dx)
+            c.set_material(sc.E, sc.nu, sc.rho)
+            c.set_plastic_alpha(sc.alpha)
+            c.add_particles(sc.position, None, sc.mass)
+            b = c.run_dynamic_body(O.collider(**sc.bodies[0].as_tuple()), sc.gravity, sc.dt, 20, ii)
+            out[kind, tag] = [np.array(b.angular_velocity[:]), np.array(b.orientation[:]), np.array(b.center[:]),
+                              c.get_particles()["position"]]
+            c.close()
+    for tag in ("identity", "tensor"):
+        for a, b in zip(out["ref", tag], out["f32", tag]):
+            assert np.array_equal(bits(a.astype(np.float32)), bits(b.astype(np.float32))), tag
+    w_id, w_t = out["ref", "identity"][0], out["ref", "tensor"][0]
+    assert np.abs(w_id).max() > 0 and np.abs(w_t - w_id).max() > 0.2 * np.abs(w_id).max()
