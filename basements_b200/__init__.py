@@ -78,6 +78,7 @@ class SceneDesc(C.Structure):
         ("body", Collider),
         ("body_dynamic", C.c_int32),
         ("body_inv_inertia", C.c_float * 9),
+        ("body_inv_inertia_given", C.c_int32),
     ]
 
 
@@ -110,6 +111,7 @@ _st = C.c_int
 
 _SIGS = {
     "bm_get_version": (C.c_int, []),
+    "bm_debug_svd3": (_st, [C.c_int64, _f, _f, _f, _f, C.c_int32]),
     "bm_status_string": (C.c_char_p, [C.c_int]),
     "bm_last_error": (C.c_char_p, []),
     "bm_set_device": (_st, [C.c_int32]),
@@ -213,6 +215,16 @@ def lib():
         f.argtypes = args
     _lib = L
     return L
+
+
+def device_svd3(F, fast_math=False):
+    """The step kernels' 3x3 SVD run on the device (bm_debug_svd3) for an
+    array of matrices F (n x 3 x 3): returns U, S (unsorted), V."""
+    F = np.ascontiguousarray(F, np.float32).reshape(-1, 3, 3)
+    U, V = np.empty_like(F), np.empty_like(F)
+    S = np.empty((len(F), 3), np.float32)
+    check(lib().bm_debug_svd3(len(F), _fp(F), _fp(U), _fp(S), _fp(V), 1 if fast_math else 0), "bm_debug_svd3")
+    return U, S, V
 
 
 def set_device(device: int):
@@ -510,6 +522,7 @@ def scene_desc(scene, keep: list) -> SceneDesc:
         d.body_dynamic = 0 if b.kinematic else 1
         if b.inv_inertia is not None:
             d.body_inv_inertia[:] = [float(v) for v in b.inv_inertia]
+            d.body_inv_inertia_given = 1
     return d
 
 

@@ -310,7 +310,7 @@ BM_API bm_status_t bm_batch_create(int32_t n_scenes, const bm_scene_desc_t* scen
             B.state = d.body;
             B.inv_mass = d.body.mass > 0.0f ? 1.0f / d.body.mass : 0.0f;
             bool zero = true;
-            for (int q = 0; q < 9; ++q) zero = zero && d.body_inv_inertia[q] == 0.0f;
+            for (int q = 0; q < 9; ++q) zero = zero && d.body_inv_inertia[q] == 0.0f && !d.body_inv_inertia_given;
             for (int q = 0; q < 9; ++q) B.inv_inertia[q] = zero ? ((q % 4 == 0) ? 1.0f : 0.0f) : d.body_inv_inertia[q];
             for (int a = 0; a < 3; ++a) B.gravity[a] = d.gravity[a];
             B.dt = d.dt;

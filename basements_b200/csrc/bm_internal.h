@@ -131,7 +131,9 @@ struct SceneDev {
     int32_t bin_shift;     // sort bins are 2^bin_shift nodes per axis (0: one cell)
     int32_t fresh;         // 1: acc[cur] holds a standalone (unfolded) P2G this step
     uint32_t* status;      // error bits
-    unsigned long long* escaped;  // [0] dropped stencil writes, [1] light-node suspects (k_grid_update)
+    // [0] dropped stencil writes, [1] light-node suspects (k_grid_update),
+    // [2] nonzero while this step's grid is being repaired (the suspects' step)
+    unsigned long long* escaped;
 };
 
 struct SceneTable {
@@ -201,10 +203,23 @@ int64_t scan_tiles(int64_t nkeys);
 // only_fresh: skip scenes whose `fresh` flag is 0 (newly admitted scenes of
 // a running table get their first P2G while the others keep theirs).
 void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st, bool only_fresh = false);
+// Exact repair of the fused kernel's light-node rule: a World's device words
+// ([0] set by the grid update when a scene found a light-node suspect, [1] a
+// count of finished CTAs of the repair) and what the repair's standalone P2G
+// needs (the table's per-particle CTAs and the current particle store).
+struct LightRepair {
+    uint32_t* word;
+    int64_t n_ctas;
+    int sel;
+    int num_sms;
+};
 // folded: acc[cur].mv holds momentum + force * dt (the force channel only
 // holds the contributions of w*m <= 1e-6 particle-node pairs); scenes whose
-// `fresh` flag is set are always treated as unfolded.
-void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st);
+// `fresh` flag is set are always treated as unfolded. With a folded grid and
+// `repair`, a scene with a light-node suspect has this step's grid redone
+// from its particles unfolded (standalone P2G, update_grid), on the device.
+void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st,
+                        const LightRepair* repair = nullptr);
 void launch_g2p(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st);
 // Fused G2P of this step + P2G of the next (into acc[1-cur]), in one of the
 // compiled launch shapes.
@@ -225,11 +240,22 @@ struct FusedScene {
     __host__ __device__ __forceinline__ float* plane(int p) const { return base + (int64_t)p * cap; }
 };
 FusedScene fused_view(const SceneDev& d, int cur, int sel);
-// Single scene, its view passed by value; many scenes, a device array of
-// views (one per scene) for this (cur, sel) and the table's CTA prefix.
+// Views of up to kPackScenes scenes and their 128-thread units, passed to the
+// many-scene fused kernel as one kernel parameter (kernel parameters of up to
+// 32,764 bytes: CUDA 12.1 and later).
+constexpr int kPackScenes = 160;
+struct FusedPack {
+    int64_t prefix[kPackScenes + 1];  // units before each scene of the pack
+    FusedScene v[kPackScenes];
+    int n;
+};
+static_assert(sizeof(FusedPack) <= 32000, "the pack fits the kernel-parameter limit");
+// Single scene, its view passed by value; many scenes, host arrays of the
+// views (one per scene) for this (cur, sel) and the table's CTA prefix: one
+// launch per pack of scenes.
 void launch_g2p2g_one(const FusedScene& scene, bool fast_math, int variant, cudaStream_t st);
-void launch_g2p2g_many(const FusedScene* d_views, const int64_t* d_prefix, int n_scenes, int64_t n_ctas,
-                       bool fast_math, int variant, cudaStream_t st);
+void launch_g2p2g_many(const FusedScene* views, const int64_t* prefix, int n_scenes, bool fast_math, int variant,
+                       cudaStream_t st);
 // Counting sort of every scene's particles by stencil base node, from
 // store[sel] into store[1-sel].
 void launch_sort(const SceneTable& t, int64_t n_ctas, int sel, const SortBuffers& sb, cudaStream_t st);
@@ -288,6 +314,9 @@ void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int6
 void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies, const int64_t* d_cand_prefix,
                     int64_t total_candidates, int cur, double* d_acc, cudaStream_t st);
 void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st);
+// Loads the code of the M1 and reaction-finalize kernels on the current
+// device (a no-op once loaded).
+cudaError_t load_m1_kernels();
 
 // Rigid bodies stepped on the device (batched and served forms), with the
 // semi-implicit Euler update of include/basements/physics/dynamics/integrator.h:19-57.

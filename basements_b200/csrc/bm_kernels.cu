@@ -85,15 +85,13 @@ __device__ __forceinline__ bool particle_slot(const SceneTable& t, int sel, PSlo
 
 // ---- standalone P2G (grid.clear() + the P2G loop) --------------------------------
 
-__global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int sel, bool only_fresh) {
-    PSlot slot;
-    if (!particle_slot(t, sel, slot)) return;
-    const SceneDev& S = t.scenes[slot.s];
-    if (only_fresh && !S.fresh) return;
+// The reference's P2G of one particle (mpm_solver.h:168-248) into acc[cur]:
+// Kirchhoff stress from the SVD of F, momentum and force kept apart (N5).
+// Returns the number of stencil writes dropped outside the box.
+__device__ __forceinline__ int p2g_particle(const SceneDev& S, int cur, int sel, int64_t p) {
     const ParticleSoA ps = S.store[sel];
     const GridDesc g = S.g;
     const GridAcc acc = S.acc[cur];
-    const int64_t p = slot.p;
     const float x[3] = {ps.plane(P_X)[p], ps.plane(P_X + 1)[p], ps.plane(P_X + 2)[p]};
     const float v[3] = {ps.plane(P_V)[p], ps.plane(P_V + 1)[p], ps.plane(P_V + 2)[p]};
     float F[9], Cm[9];
@@ -146,21 +144,78 @@ __global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int
                 red_v4(acc.f + id, s0 * w, s1 * w, s2 * w, 0.0f);
             }
     mark_stencil_blocks(g, acc, S.alloc, base, wgt[0], wgt[1], wgt[2]);
-    report(S, dropped, true);
+    return dropped;
+}
+
+__global__ void __launch_bounds__(kParticleCTA) k_p2g(SceneTable t, int cur, int sel, bool only_fresh) {
+    PSlot slot;
+    if (!particle_slot(t, sel, slot)) return;
+    const SceneDev& S = t.scenes[slot.s];
+    if (only_fresh && !S.fresh) return;
+    report(S, p2g_particle(S, cur, sel, slot.p), true);
 }
 
 // ---- grid update -------------------------------------------------------------------
+
+// update_grid (mpm_solver.h:250-291) of node tt of listed block b of acc c.
+// folded: the momentum already holds force * dt (the fused kernel's P2G).
+__device__ __forceinline__ void update_node(const GridDesc& g, const GridAcc& c, const Material& mat, float dt,
+                                            bool folded, int64_t b, int tt) {
+    const int64_t id = g.node_of_block(b, tt);
+    const float4 mv = c.mv[id];
+    if (!(mv.w > 1e-6f)) {
+        // inactive (mass 0) or mass <= 1e-6: the reference leaves the
+        // momentum (without force) in place (mpm_solver.h:257)
+        if (folded && (mv.w > 0.0f || mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f)) {
+            const float4 f = c.f[id];
+            c.mv[id] = make_float4(mv.x - f.x * dt, mv.y - f.y * dt, mv.z - f.z * dt, mv.w);
+        }
+        return;
+    }
+    float v0, v1, v2;
+    if (folded) {
+        v0 = mv.x / mv.w;
+        v1 = mv.y / mv.w;
+        v2 = mv.z / mv.w;
+    } else {
+        const float4 f = c.f[id];
+        v0 = (mv.x + f.x * dt) / mv.w;
+        v1 = (mv.y + f.y * dt) / mv.w;
+        v2 = (mv.z + f.z * dt) / mv.w;
+    }
+    v0 = v0 + mat.gx * dt;
+    v1 = v1 + mat.gy * dt;
+    v2 = v2 + mat.gz * dt;
+    const int lj = (tt >> 2) & 3;
+    const int bj = (int)((b / g.nbz) % g.nby);
+    const int j = g.oy + 4 * bj + lj;
+    const float node_y = ((float)j + 0.5f) * g.dx;
+    if (node_y < g.dx && v1 < 0.0f) {
+        const float vn = -v1;
+        v1 = 0.0f;
+        const float mag = sqrtf(v0 * v0 + v2 * v2);
+        const float budget = mat.floor_friction * vn;
+        if (mag > 1e-12f) {
+            const float sc = smax(0.0f, (mag - budget) / mag);
+            v0 = v0 * sc;
+            v2 = v2 * sc;
+        }
+    }
+    c.mv[id] = make_float4(v0, v1, v2, mv.w);
+}
 
 // update_grid over the blocks listed in acc[cur] of scene blockIdx.y (every
 // other node of the box is empty, so skipping it is exact); the same launch
 // zeroes the blocks listed in acc[1-cur] so that it can take the next P2G.
 // Before zeroing a node of acc[1-cur] (the previous step's grid, particle
-// mass in .w) it counts the node as a light-node suspect when that mass was
-// at least kHeavyNodeMass and the node's new particle mass in a folded
-// acc[cur] is in (0, 1e-6]: only there can the fused kernel have skipped a
-// force record that update_grid needs (the mass lane of acc[cur] is not
-// changed by this launch).
-__global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int cur, bool folded_all) {
+// mass in .w) it looks for light-node suspects: nodes whose particle mass
+// was at least kHeavyNodeMass there and is in (0, 1e-6] in a folded
+// acc[cur]. Only at such a node can the fused kernel have skipped a force
+// record that update_grid needs (the mass lane of acc[cur] is not changed by
+// this launch). A suspect is counted (escaped[1]) and marks its scene for
+// the repair that follows (escaped[2], and repair[0] for the launch).
+__global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int cur, bool folded_all,
+                                                              uint32_t* repair) {
     const SceneDev& S = t.scenes[blockIdx.y];
     const bool folded = folded_all && !S.fresh;
     const GridDesc g = S.g;
@@ -176,55 +231,86 @@ __global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int 
             const int64_t id = g.node_of_block(b, tt);
             if (folded && o.mv[id].w >= kHeavyNodeMass) {
                 const float m_new = c.mv[id].w;
-                if (m_new > 0.0f && m_new <= 1e-6f) atomicAdd(S.escaped + 1, 1ull);
+                if (m_new > 0.0f && m_new <= 1e-6f) {
+                    atomicAdd(S.escaped + 1, 1ull);
+                    S.escaped[2] = 1ull;
+                    if (repair) *repair = 1u;
+                }
             }
             o.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
             o.f[id] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (tt == 0) o.touched[b] = 0u;
             continue;
         }
-        const int64_t b = c.list[slot];
-        const int64_t id = g.node_of_block(b, tt);
-        const float4 mv = c.mv[id];
-        if (!(mv.w > 1e-6f)) {
-            // inactive (mass 0) or mass <= 1e-6: the reference leaves the
-            // momentum (without force) in place (mpm_solver.h:257)
-            if (folded && (mv.w > 0.0f || mv.x != 0.0f || mv.y != 0.0f || mv.z != 0.0f)) {
-                const float4 f = c.f[id];
-                c.mv[id] = make_float4(mv.x - f.x * dt, mv.y - f.y * dt, mv.z - f.z * dt, mv.w);
-            }
-            continue;
-        }
-        float v0, v1, v2;
-        if (folded) {
-            v0 = mv.x / mv.w;
-            v1 = mv.y / mv.w;
-            v2 = mv.z / mv.w;
-        } else {
-            const float4 f = c.f[id];
-            v0 = (mv.x + f.x * dt) / mv.w;
-            v1 = (mv.y + f.y * dt) / mv.w;
-            v2 = (mv.z + f.z * dt) / mv.w;
-        }
-        v0 = v0 + mat.gx * dt;
-        v1 = v1 + mat.gy * dt;
-        v2 = v2 + mat.gz * dt;
-        const int lj = (tt >> 2) & 3;
-        const int bj = (int)((b / g.nbz) % g.nby);
-        const int j = g.oy + 4 * bj + lj;
-        const float node_y = ((float)j + 0.5f) * g.dx;
-        if (node_y < g.dx && v1 < 0.0f) {
-            const float vn = -v1;
-            v1 = 0.0f;
-            const float mag = sqrtf(v0 * v0 + v2 * v2);
-            const float budget = mat.floor_friction * vn;
-            if (mag > 1e-12f) {
-                const float sc = smax(0.0f, (mag - budget) / mag);
-                v0 = v0 * sc;
-                v2 = v2 * sc;
-            }
-        }
-        c.mv[id] = make_float4(v0, v1, v2, mv.w);
+        update_node(g, c, mat, dt, folded, c.list[slot], tt);
+    }
+}
+
+// ---- exact repair of the light-node rule -----------------------------------------
+//
+// A scene marked by k_grid_update redoes this step's grid from its particles:
+// acc[cur] is zeroed on its listed blocks (the list and the block flags
+// stay), the standalone P2G (momentum and force apart, stress from the SVD
+// of F as in the reference) refills it, and update_grid runs unfolded. The
+// result is the reference's grid for that step, N2 nodes included. Each
+// kernel returns at once when repair[0] is 0, the case of every step whose
+// scenes saw no suspect. The clear kernel also resets the counts of
+// acc[1-cur] that k_grid_update has just zeroed.
+
+__global__ void __launch_bounds__(kGridThreads) k_repair_clear(SceneTable t, int cur, const uint32_t* repair) {
+    const SceneDev& S = t.scenes[blockIdx.y];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *S.acc[1 - cur].count = 0;
+    if (*repair == 0u || S.escaped[2] == 0ull) return;
+    const GridDesc g = S.g;
+    const GridAcc c = S.acc[cur];
+    const int64_t total = (int64_t)(*c.count) * 64;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t id = g.node_of_block(c.list[e >> 6], (int)(e & 63));
+        c.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+        c.f[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// Standalone P2G of the marked scenes, CTAs striding over the table's
+// 128-particle units (stencil writes outside the box were already counted by
+// the fused kernel, so they are not counted again).
+__global__ void __launch_bounds__(kParticleCTA) k_repair_p2g(SceneTable t, int cur, int sel, const uint32_t* repair) {
+    if (*repair == 0u) return;
+    const int64_t units = t.cta_prefix[t.n_scenes];
+    for (int64_t unit = blockIdx.x; unit < units; unit += gridDim.x) {
+        const int s = scene_of_cta(t, unit);
+        const SceneDev& S = t.scenes[s];
+        if (S.escaped[2] == 0ull) continue;
+        const int64_t p = (unit - t.cta_prefix[s]) * kParticleCTA + threadIdx.x;
+        if (p < S.store[sel].n) p2g_particle(S, cur, sel, p);
+    }
+}
+
+// Unfolded update_grid of the marked scenes; the last CTA to finish clears
+// the marks for the next step.
+__global__ void __launch_bounds__(kGridThreads) k_repair_update(SceneTable t, int cur, uint32_t* repair) {
+    if (*repair == 0u) return;
+    const SceneDev& S = t.scenes[blockIdx.y];
+    if (S.escaped[2] != 0ull) {
+        const GridAcc c = S.acc[cur];
+        const int64_t total = (int64_t)(*c.count) * 64;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+             e += (int64_t)gridDim.x * blockDim.x)
+            update_node(S.g, c, S.mat, S.dt, false, c.list[e >> 6], (int)(e & 63));
+    }
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(repair + 1, 1u) == gridDim.x * gridDim.y - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    for (int s = threadIdx.x; s < t.n_scenes; s += blockDim.x) t.scenes[s].escaped[2] = 0ull;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        repair[1] = 0u;
+        repair[0] = 0u;
     }
 }
 
@@ -606,35 +692,28 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
     }
 }
 
-// Many scenes: the view of each 128-thread unit's scene comes from the CTA
-// prefix table. Every unit belongs to one scene; its first thread copies the
-// view into shared memory, so the scene's fields are read from there (a view
-// read through a global pointer stays live in registers and made this kernel
-// spill four to six times more than the single-scene one).
+// Many scenes: the views of up to kPackScenes scenes travel as one kernel
+// parameter (FusedPack), so that, as in the single-scene kernel, every field
+// of a scene is read through the constant bank rather than from memory. A
+// 128-thread unit finds its scene by a binary search of the pack's prefix;
+// with 128-thread CTAs the scene index is uniform over the CTA, and the
+// fields can sit in uniform registers. (An earlier form copied each unit's
+// view into shared memory: its fields were reloaded from there throughout the
+// particle, short-scoreboard waits 2.75 per issue against 0.67 for the
+// constant bank, and about 150 more instructions per particle.)
 template <bool Fast, int Threads, int MinBlocks>
-__global__ void __launch_bounds__(Threads, MinBlocks)
-    k_g2p2g(const FusedScene* __restrict__ views, const int64_t* __restrict__ prefix, int n_scenes) {
-    constexpr int kUnitThreads = Threads < kParticleCTA ? Threads : kParticleCTA;
-    constexpr int kUnits = Threads / kUnitThreads;
-    __shared__ FusedScene sview[kUnits];
-    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(Threads, MinBlocks) k_g2p2g_pack(const __grid_constant__ FusedPack P) {
+    const int64_t gtid = (int64_t)blockIdx.x * Threads + threadIdx.x;
     const int64_t unit = gtid / kParticleCTA;
-    const int u = (int)threadIdx.x / kUnitThreads;
-    const bool live = unit < prefix[n_scenes];
-    int lo = 0;
-    if (live) {
-        int hi = n_scenes - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (prefix[mid] <= unit) lo = mid;
-            else hi = mid - 1;
-        }
-        if (threadIdx.x % kUnitThreads == 0) sview[u] = views[lo];
+    if (unit >= P.prefix[P.n]) return;
+    int lo = 0, hi = P.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.prefix[mid] <= unit) lo = mid;
+        else hi = mid - 1;
     }
-    __syncthreads();
-    if (!live) return;
-    const int64_t p = (unit - prefix[lo]) * kParticleCTA + (gtid % kParticleCTA);
-    const FusedScene& S = sview[u];
+    const FusedScene& S = P.v[lo];
+    const int64_t p = (unit - P.prefix[lo]) * kParticleCTA + (gtid % kParticleCTA);
     if (p >= S.n) return;
     g2p2g_particle<Fast>(S, p);
 }
@@ -836,12 +915,13 @@ inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 struct FusedVariant {
     const char* name;
     int threads;
-    void (*fn[2])(const FusedScene*, const int64_t*, int);
+    void (*pack[2])(const FusedPack);
     void (*one[2])(const FusedScene);
 };
 
-#define BM_FUSED(T, B)                                                                               \
-    {#T "x" #B, T, {k_g2p2g<false, T, B>, k_g2p2g<true, T, B>}, {k_g2p2g_one<false, T, B>, k_g2p2g_one<true, T, B>}}
+#define BM_FUSED(T, B)                                                                       \
+    {#T "x" #B, T, {k_g2p2g_pack<false, T, B>, k_g2p2g_pack<true, T, B>},                   \
+     {k_g2p2g_one<false, T, B>, k_g2p2g_one<true, T, B>}}
 const FusedVariant kFused[] = {
     BM_FUSED(128, 4), BM_FUSED(128, 5), BM_FUSED(128, 6), BM_FUSED(256, 2), BM_FUSED(256, 3), BM_FUSED(64, 10),
     BM_FUSED(128, 8), BM_FUSED(128, 7),
@@ -861,13 +941,24 @@ void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStrea
     k_p2g<<<(unsigned)n_ctas, kParticleCTA, 0, st>>>(t, cur, sel, only_fresh);
 }
 
-void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st) {
+void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st,
+                        const LightRepair* repair) {
     if (t.n_scenes <= 0) return;
     const int64_t want = (2 * max_blocks * 64 + kGridThreads - 1) / kGridThreads;
     const int64_t cap = std::max<int64_t>(4, 148 * 8 / t.n_scenes);
     const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, cap));
-    k_grid_update<<<dim3(gx, (unsigned)t.n_scenes), kGridThreads, 0, st>>>(t, cur, folded);
-    k_reset_counts<<<nblk(t.n_scenes, 128), 128, 0, st>>>(t, 1 - cur);
+    const dim3 grid(gx, (unsigned)t.n_scenes);
+    k_grid_update<<<grid, kGridThreads, 0, st>>>(t, cur, folded, folded && repair ? repair->word : nullptr);
+    if (!folded || !repair) {
+        k_reset_counts<<<nblk(t.n_scenes, 128), 128, 0, st>>>(t, 1 - cur);
+        return;
+    }
+    k_repair_clear<<<grid, kGridThreads, 0, st>>>(t, cur, repair->word);
+    if (repair->n_ctas > 0) {
+        const int64_t ctas = std::min<int64_t>(repair->n_ctas, (int64_t)repair->num_sms * 8);
+        k_repair_p2g<<<(unsigned)ctas, kParticleCTA, 0, st>>>(t, cur, repair->sel, repair->word);
+    }
+    k_repair_update<<<grid, kGridThreads, 0, st>>>(t, cur, repair->word);
 }
 
 void launch_g2p(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st) {
@@ -899,12 +990,24 @@ void launch_g2p2g_one(const FusedScene& scene, bool fast_math, int variant, cuda
     v.one[fast_math ? 1 : 0]<<<nblk(scene.n, v.threads), v.threads, 0, st>>>(scene);
 }
 
-void launch_g2p2g_many(const FusedScene* d_views, const int64_t* d_prefix, int n_scenes, int64_t n_ctas,
-                       bool fast_math, int variant, cudaStream_t st) {
-    if (n_ctas <= 0 || n_scenes <= 0) return;
+void launch_g2p2g_many(const FusedScene* views, const int64_t* prefix, int n_scenes, bool fast_math, int variant,
+                       cudaStream_t st) {
+    if (n_scenes <= 0) return;
     const FusedVariant& v = kFused[(variant >= 0 && variant < kNumFused) ? variant : 0];
-    v.fn[fast_math ? 1 : 0]<<<nblk(n_ctas * kParticleCTA, v.threads), v.threads, 0, st>>>(d_views, d_prefix,
-                                                                                         n_scenes);
+    // one launch per pack of up to kPackScenes consecutive scenes
+    static thread_local FusedPack pack;
+    for (int first = 0; first < n_scenes; first += kPackScenes) {
+        const int n = std::min(kPackScenes, n_scenes - first);
+        const int64_t units = prefix[first + n] - prefix[first];
+        if (units <= 0) continue;
+        pack.n = n;
+        for (int q = 0; q < n; ++q) {
+            pack.v[q] = views[first + q];
+            pack.prefix[q] = prefix[first + q] - prefix[first];
+        }
+        pack.prefix[n] = units;
+        v.pack[fast_math ? 1 : 0]<<<nblk(units * kParticleCTA, v.threads), v.threads, 0, st>>>(pack);
+    }
 }
 
 void launch_sort(const SceneTable& t, int64_t n_ctas, int sel, const SortBuffers& sb, cudaStream_t st) {

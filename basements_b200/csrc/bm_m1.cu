@@ -640,6 +640,15 @@ void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies,
     k_m1<<<(unsigned)total_candidates, 64, 0, st>>>(t, d_params, cur, d_acc, d_cand_prefix, n_bodies);
 }
 
+cudaError_t load_m1_kernels() {
+    // under CUDA's lazy module loading a kernel's code is loaded on its first
+    // use, and querying its attributes is such a use
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, k_m1);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_reaction_finalize);
+    return e;
+}
+
 void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st) {
     if (n_bodies <= 0) return;
     k_reaction_finalize<<<nblk(n_bodies, 64), 64, 0, st>>>(d_acc, n_bodies, d_out);

@@ -175,7 +175,7 @@ bm_status_t rebuild_bodies(bm_server* s, const std::vector<int>& old_body) {
         B.state = r.desc.body;
         B.inv_mass = r.desc.body.mass > 0.0f ? 1.0f / r.desc.body.mass : 0.0f;
         bool zero = true;
-        for (int q = 0; q < 9; ++q) zero = zero && r.desc.body_inv_inertia[q] == 0.0f;
+        for (int q = 0; q < 9; ++q) zero = zero && r.desc.body_inv_inertia[q] == 0.0f && !r.desc.body_inv_inertia_given;
         for (int q = 0; q < 9; ++q)
             B.inv_inertia[q] = zero ? ((q % 4 == 0) ? 1.0f : 0.0f) : r.desc.body_inv_inertia[q];
         for (int c = 0; c < 3; ++c) B.gravity[c] = r.desc.gravity[c];

@@ -234,6 +234,8 @@ void invalidate_state(bm_solver* s) {
     s->sorted = false;
 }
 
+bm_status_t noalloc_setup(int dev);  // defined with the no-alloc coupler below
+
 }  // namespace sol
 }  // namespace bm
 
@@ -295,6 +297,7 @@ BM_API bm_status_t bm_solver_create(float dx, const bm_domain_t* domain, bm_solv
         h.domain_set = true;
     }
     st = ensure_reactions(s, 4);
+    if (st == BM_OK) st = noalloc_setup(s->w.device);
     if (st != BM_OK) {
         bm_solver_destroy(s);
         return st;
@@ -797,9 +800,12 @@ BM_API const char* bm_launch_variant_name(int32_t variant) { return fused_varian
 //
 // The array is shared by every solver on a device. Two calls that overlap in
 // time (from two host threads, on any streams) race on it and give wrong
-// reactions; callers must serialise them. The first call on each device looks
-// up the array's device address (cudaGetSymbolAddress) and keeps it; make that
-// first call before any stream capture begins on that device.
+// reactions; callers must serialise them. Its device address is looked up
+// (cudaGetSymbolAddress) and the M1 kernels are loaded once per device by
+// bm_solver_create, a call that allocates anyway: under CUDA's default lazy
+// module loading, the first lookup of the array or launch of a kernel loads
+// code and may allocate device memory, so leaving them to the first no-alloc
+// call would allocate in the one call that must not.
 
 namespace {
 
@@ -830,9 +836,11 @@ bm_status_t noalloc_scratch(int dev, unsigned char** out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_ptr[dev]) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_m1_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            set_last_error(std::string("cudaGetSymbolAddress(no-alloc M1 scratch): ") + cudaGetErrorString(e));
+        cudaError_t e = cudaGetSymbolAddress(&p, g_m1_noalloc_scratch);
+        if (e == cudaSuccess && !p) e = cudaErrorInvalidSymbol;
+        if (e == cudaSuccess) e = load_m1_kernels();
+        if (e != cudaSuccess) {
+            set_last_error(std::string("no-alloc M1 set-up (scratch address, kernel load): ") + cudaGetErrorString(e));
             return BM_ERR_CUDA;
         }
         g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
@@ -842,6 +850,17 @@ bm_status_t noalloc_scratch(int dev, unsigned char** out) {
 }
 
 }  // namespace
+
+namespace bm {
+namespace sol {
+// Set-up of bm_coupler_m1_apply_noalloc on the current device, from
+// bm_solver_create.
+bm_status_t noalloc_setup(int dev) {
+    unsigned char* p = nullptr;
+    return noalloc_scratch(dev, &p);
+}
+}  // namespace sol
+}  // namespace bm
 
 BM_API bm_status_t bm_coupler_m1_apply_noalloc(bm_solver_t* s, int32_t n_bodies, const bm_collider_t* bodies,
                                                float dt, bm_reaction_t* out) {

@@ -190,30 +190,53 @@ bm_status_t World::init() {
     BM_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     BM_CHECK_CUDA(cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking));
     BM_CHECK_CUDA(cudaEventCreateWithFlags(&upload_done, cudaEventDisableTiming));
-    for (auto& e : stage_used) BM_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    BM_CHECK_CUDA(cudaMalloc((void**)&d_repair, 2 * sizeof(uint32_t)));
+    BM_CHECK_CUDA(cudaMemsetAsync(d_repair, 0, 2 * sizeof(uint32_t), stream));
     return BM_OK;
 }
 
 bm_status_t World::stage_begin(size_t bytes, void** out) {
-    const int k = stage_next;
-    BM_CHECK_CUDA(cudaEventSynchronize(stage_used[k]));  // the copies that last read this buffer ran
-    if (stage_cap[k] < bytes) {
-        give_stage_block(stage_buf[k], stage_cap[k]);
-        stage_buf[k] = nullptr;
-        stage_cap[k] = 0;
-        if (!take_stage_block(bytes, &stage_buf[k], &stage_cap[k])) {
+    // a slot whose copies have run (an event never recorded counts as done),
+    // searched from the one after the last handed out
+    const int n = (int)stage.size();
+    int k = -1;
+    for (int q = 0; q < n && k < 0; ++q) {
+        const int c = (stage_next + q) % n;
+        const cudaError_t e = cudaEventQuery(stage[c].used);
+        if (e == cudaSuccess) k = c;
+        else if (e != cudaErrorNotReady) BM_CHECK_CUDA(e);
+    }
+    if (k < 0 && n < kMaxStageSlots) {
+        StageSlot slot;
+        BM_CHECK_CUDA(cudaEventCreateWithFlags(&slot.used, cudaEventDisableTiming));
+        stage.push_back(slot);
+        k = n;
+    }
+    if (k < 0) {  // every slot in flight: wait for the next in turn
+        k = stage_next % n;
+        BM_CHECK_CUDA(cudaEventSynchronize(stage[k].used));
+    }
+    StageSlot& sl = stage[k];
+    if (sl.cap < bytes) {
+        give_stage_block(sl.buf, sl.cap);
+        sl.buf = nullptr;
+        sl.cap = 0;
+        if (!take_stage_block(bytes, &sl.buf, &sl.cap)) {
             const size_t cap = std::max<size_t>(bytes * 2, 1 << 16);
-            BM_CHECK_CUDA(cudaMallocHost(&stage_buf[k], cap));
-            stage_cap[k] = cap;
+            BM_CHECK_CUDA(cudaMallocHost(&sl.buf, cap));
+            sl.cap = cap;
         }
     }
-    *out = stage_buf[k];
+    stage_cur = k;
+    *out = sl.buf;
     return BM_OK;
 }
 
 void World::stage_done() {
-    cudaEventRecord(stage_used[stage_next], stream);
-    stage_next ^= 1;
+    if (stage_cur < 0) return;
+    cudaEventRecord(stage[stage_cur].used, stream);
+    stage_next = (stage_cur + 1) % (int)stage.size();
+    stage_cur = -1;
 }
 
 void World::free_scene(SceneHost& h) {
@@ -253,11 +276,6 @@ void World::release() {
     scenes.clear();
     cudaFree(d_scenes);
     cudaFree(d_prefix);
-    for (auto& r : d_views)
-        for (auto& v : r) {
-            cudaFree(v);
-            v = nullptr;
-        }
     cudaFree(sort.count);
     cudaFree(sort.start);
     cudaFree(sort.tile_sum);
@@ -276,17 +294,21 @@ void World::release() {
     t0 = t1 = nullptr;
     if (stream) cudaStreamSynchronize(stream);
     if (upload) cudaStreamSynchronize(upload);
+    for (auto& sl : stage) {
+        give_stage_block(sl.buf, sl.cap);  // the streams are idle: no copy reads it
+        if (sl.used) cudaEventDestroy(sl.used);
+    }
+    stage.clear();
+    stage_next = 0;
+    stage_cur = -1;
     for (int k = 0; k < 2; ++k) {
-        give_stage_block(stage_buf[k], stage_cap[k]);  // the streams are idle: no copy reads it
-        stage_buf[k] = nullptr;
-        stage_cap[k] = 0;
-        if (stage_used[k]) cudaEventDestroy(stage_used[k]);
-        stage_used[k] = nullptr;
         if (read_done[k]) cudaEventDestroy(read_done[k]);
         read_done[k] = nullptr;
     }
     if (upload_done) cudaEventDestroy(upload_done);
     upload_done = nullptr;
+    cudaFree(d_repair);
+    d_repair = nullptr;
     if (upload) cudaStreamDestroy(upload);
     upload = nullptr;
     if (stream) cudaStreamDestroy(stream);
@@ -310,9 +332,9 @@ bm_status_t World::p2g_fresh() {
 int World::add_scene() {
     scenes.emplace_back();
     SceneHost& h = scenes.back();
-    if (dmalloc(&h.dev.status, 1, stream, pool) == BM_OK && dmalloc(&h.dev.escaped, 2, stream, pool) == BM_OK) {
+    if (dmalloc(&h.dev.status, 1, stream, pool) == BM_OK && dmalloc(&h.dev.escaped, 3, stream, pool) == BM_OK) {
         cudaMemsetAsync(h.dev.status, 0, sizeof(uint32_t), stream);
-        cudaMemsetAsync(h.dev.escaped, 0, 2 * sizeof(unsigned long long), stream);
+        cudaMemsetAsync(h.dev.escaped, 0, 3 * sizeof(unsigned long long), stream);
     }
     dirty = true;
     return (int)scenes.size() - 1;
@@ -564,12 +586,6 @@ bm_status_t World::sync_table() {
         const size_t cap = std::max<size_t>(ns, table_cap * 2);
         BM_CHECK_CUDA(cudaMalloc((void**)&d_scenes, sizeof(SceneDev) * cap));
         BM_CHECK_CUDA(cudaMalloc((void**)&d_prefix, sizeof(int64_t) * (cap + 1)));
-        for (auto& r : d_views)
-            for (auto& v : r) {
-                cudaFree(v);
-                v = nullptr;
-                BM_CHECK_CUDA(cudaMalloc((void**)&v, sizeof(FusedScene) * cap));
-            }
         table_cap = cap;
     }
     if (keys > sort_cap) {
@@ -583,26 +599,23 @@ bm_status_t World::sync_table() {
         sort_cap = cap;
     }
     sort.nkeys = keys;
+    for (int c = 0; c < 2; ++c)
+        for (int p = 0; p < 2; ++p) {
+            h_views[c][p].resize(ns);
+            for (int q = 0; q < ns; ++q) h_views[c][p][q] = fused_view(host[q], c, p);
+        }
     if (ns > 0) {
-        // one pinned staging buffer: 4 view tables, the scene table, the prefix
+        // one pinned staging buffer: the scene table, the prefix
         auto up16 = [](size_t b) { return (b + 15) & ~size_t(15); };
-        const size_t vb = up16(sizeof(FusedScene) * ns), sb = up16(sizeof(SceneDev) * ns),
-                     pb = sizeof(int64_t) * (ns + 1);
+        const size_t sb = up16(sizeof(SceneDev) * ns), pb = sizeof(int64_t) * (ns + 1);
         void* buf = nullptr;
-        bm_status_t st = stage_begin(4 * vb + sb + pb, &buf);
+        bm_status_t st = stage_begin(sb + pb, &buf);
         if (st != BM_OK) return st;
         char* b = static_cast<char*>(buf);
-        for (int c = 0; c < 2; ++c)
-            for (int p = 0; p < 2; ++p) {
-                FusedScene* views = reinterpret_cast<FusedScene*>(b + (2 * c + p) * vb);
-                for (int q = 0; q < ns; ++q) views[q] = fused_view(host[q], c, p);
-                BM_CHECK_CUDA(cudaMemcpyAsync(d_views[c][p], views, sizeof(FusedScene) * ns, cudaMemcpyHostToDevice,
-                                              stream));
-            }
-        std::memcpy(b + 4 * vb, host.data(), sizeof(SceneDev) * ns);
-        std::memcpy(b + 4 * vb + sb, prefix.data(), pb);
-        BM_CHECK_CUDA(cudaMemcpyAsync(d_scenes, b + 4 * vb, sizeof(SceneDev) * ns, cudaMemcpyHostToDevice, stream));
-        BM_CHECK_CUDA(cudaMemcpyAsync(d_prefix, b + 4 * vb + sb, pb, cudaMemcpyHostToDevice, stream));
+        std::memcpy(b, host.data(), sizeof(SceneDev) * ns);
+        std::memcpy(b + sb, prefix.data(), pb);
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_scenes, b, sizeof(SceneDev) * ns, cudaMemcpyHostToDevice, stream));
+        BM_CHECK_CUDA(cudaMemcpyAsync(d_prefix, b + sb, pb, cudaMemcpyHostToDevice, stream));
         stage_done();
     }
     dirty = false;
@@ -626,7 +639,8 @@ bm_status_t World::clear_and_p2g() {
 }
 
 bm_status_t World::update(bool folded) {
-    timed("grid_update", [&] { launch_grid_update(table(), max_blocks(), cur, folded, stream); });
+    const LightRepair repair{d_repair, n_ctas(), sel, num_sms};
+    timed("grid_update", [&] { launch_grid_update(table(), max_blocks(), cur, folded, stream, &repair); });
     return launch_status("grid_update");
 }
 
@@ -642,7 +656,8 @@ bm_status_t World::g2p2g(bool fast_math, int variant) {
             d.mat = material(scenes[0]);
             launch_g2p2g_one(fused_view(d, cur, sel), fast_math, variant, stream);
         } else {
-            launch_g2p2g_many(d_views[cur][sel], d_prefix, (int)scenes.size(), n_ctas(), fast_math, variant, stream);
+            launch_g2p2g_many(h_views[cur][sel].data(), prefix.data(), (int)scenes.size(), fast_math, variant,
+                              stream);
         }
     });
     cur = 1 - cur;

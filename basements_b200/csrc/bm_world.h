@@ -60,16 +60,28 @@ public:
     // stream, ordered before the compute stream's next kernel by an event.
     cudaStream_t upload = nullptr;
     cudaEvent_t upload_done = nullptr;
-    // Pinned, double-buffered staging for small uploads on `stream` (the scene
-    // table): a buffer is rewritten only after the copies that read it ran.
-    void* stage_buf[2] = {nullptr, nullptr};
-    size_t stage_cap[2] = {0, 0};
-    cudaEvent_t stage_used[2] = {nullptr, nullptr};
-    int stage_next = 0;
+    // Pinned staging for small uploads on `stream` (the scene table, the
+    // served form's body arrays): a ring of slots, each rewritten only after
+    // the copies that read it ran. Those copies wait on the stream behind the
+    // work already enqueued, so a slot stays busy for as long as the GPU lags
+    // the host; the ring takes any slot whose copies have landed and grows
+    // (up to kMaxStageSlots) instead of waiting for one.
+    struct StageSlot {
+        void* buf = nullptr;
+        size_t cap = 0;
+        cudaEvent_t used = nullptr;
+    };
+    static constexpr int kMaxStageSlots = 32;
+    std::vector<StageSlot> stage;
+    int stage_next = 0;  // where the search for a free slot starts
+    int stage_cur = -1;  // slot handed out by the last stage_begin
     // Events of the pinned chunk pair through which read_fields brings
     // particle rows back into pageable host arrays and upload_bytes sends
     // them up.
     cudaEvent_t read_done[2] = {nullptr, nullptr};
+    // Device words of the light-node repair (LightRepair::word), zero between
+    // steps.
+    uint32_t* d_repair = nullptr;
     std::vector<SceneHost> scenes;
     int cur = 0;  // accumulation buffer of the current step
     int sel = 0;  // current particle store
@@ -82,7 +94,9 @@ public:
     bool dirty = true;
     SortBuffers sort{};
     int64_t sort_cap = 0;
-    FusedScene* d_views[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][sel]
+    // The fused kernel's view of every scene for each (cur, sel), on the host:
+    // the many-scene kernel takes them as a kernel parameter.
+    std::vector<FusedScene> h_views[2][2];
 
     // Profiling with CUDA events on the stream.
     bool profiling = false;

@@ -34,7 +34,7 @@ extern "C" {
 #define BM_API __attribute__((visibility("default")))
 #endif
 
-#define BM_API_VERSION 1
+#define BM_API_VERSION 2
 
 typedef enum bm_status {
     BM_OK = 0,
@@ -176,8 +176,10 @@ BM_API bm_status_t bm_coupler_m1_apply(bm_solver_t* s, const bm_collider_t* body
  * a pool already holds. n_bodies > 64 gives BM_ERR_INVALID_ARGUMENT; calling it
  * before bm_solver_p2g + bm_solver_grid_update have built the grid gives
  * BM_ERR_STATE. The array is shared by all solvers on a device: calls that
- * overlap in time race on it, so serialise them. The first call on a device
- * looks up the array's address; make it before any stream capture begins.
+ * overlap in time race on it, so serialise them. bm_solver_create looks up
+ * the array's address and loads the M1 kernels on its device: under CUDA's
+ * default lazy module loading that first use loads code and may allocate
+ * device memory, which the create call is allowed to do and this one is not.
  * `out` (n_bodies entries) is written before the call returns. */
 BM_API bm_status_t bm_coupler_m1_apply_noalloc(bm_solver_t* s, int32_t n_bodies, const bm_collider_t* bodies,
                                                float dt, bm_reaction_t* out);
@@ -310,8 +312,10 @@ typedef struct bm_scene_desc {
     int32_t has_body;
     bm_collider_t body;
     int32_t body_dynamic;        /* 0: kinematic (moved by its velocities only) */
-    float body_inv_inertia[9];   /* body-space inverse inertia; all zero = identity,
-                                    the reference scenes' value (integrator.h:33) */
+    float body_inv_inertia[9];   /* body-space inverse inertia (integrator.h:33) */
+    int32_t body_inv_inertia_given; /* 1: body_inv_inertia as given, all zero included
+                                       (a body that cannot rotate); 0: all zero means
+                                       the identity, the reference scenes' value */
 } bm_scene_desc_t;
 
 typedef struct bm_batch bm_batch_t;
@@ -446,6 +450,14 @@ BM_API bm_status_t bm_adjoint_backward_state(bm_tape_t* t, const bm_particles_vi
 /* dL/d(body linear velocity) and dL/d(body angular velocity) of every step
  * of the last backward pass: n_steps x 6 doubles. */
 BM_API bm_status_t bm_tape_body_grad(bm_tape_t* t, int32_t n_steps, double* out);
+
+/* ---- test support ----------------------------------------------------- */
+/* SVD::compute (include/basements/core/math/svd.h:18-108) as the step kernels
+ * run it on the device, for n row-major 3x3 matrices F (host arrays): U, V
+ * (n x 9) and the unsorted singular values S (n x 3). fast_math selects the
+ * fast-intrinsic arithmetic of bm_solver_set_math_mode. Synchronous; it
+ * allocates device memory for the call. */
+BM_API bm_status_t bm_debug_svd3(int64_t n, const float* F, float* U, float* S, float* V, int32_t fast_math);
 
 #ifdef __cplusplus
 }

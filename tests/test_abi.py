@@ -38,7 +38,7 @@ def test_python_bindings_cover_header():
 
 def test_version_and_status_strings():
     L = bm.lib()
-    assert L.bm_get_version() == 1
+    assert L.bm_get_version() == 2
     for code in range(10):
         assert L.bm_status_string(code)
     assert L.bm_status_string(999) == b"unknown status"

@@ -150,3 +150,28 @@ def test_device_body_update_with_inverse_inertia_matches_reference():
     np.testing.assert_allclose(gb.linear_velocity[:], body.linear_velocity[:], atol=2e-4)
     np.testing.assert_allclose(gb.center[:], body.center[:], atol=1e-5)
     np.testing.assert_allclose(gb.orientation[:], body.orientation[:], atol=1e-5)
+
+
+def test_device_body_with_zero_inverse_inertia_does_not_rotate():
+    """A body given an all-zero inverse inertia (infinite inertia: the
+    reference integrator's w += I^-1 tau dt leaves its spin alone,
+    integrator.h:34) keeps its spin and orientation on the device, as in the
+    reference run with the same tensor; the unset tensor still means the
+    identity, which spins the same box."""
+    zero = np.zeros((3, 3), np.float32)
+    sc = scenes.pressed_box(zero)
+    steps = 20
+    b = bm.Batch([sc, scenes.pressed_box()])
+    b.step(steps)
+    assert b.sync()[0] == 0
+    c = O.CpuSolver(REF, sc.dx)
+    c.set_material(sc.E, sc.nu, sc.rho)
+    c.set_plastic_alpha(sc.alpha)
+    c.add_particles(sc.position, None, sc.mass)
+    body = c.run_dynamic_body(O.collider(**sc.bodies[0].as_tuple()), sc.gravity, sc.dt, steps, zero)
+    gb, spun = b.get_body(0), b.get_body(1)
+    assert np.array_equal(gb.angular_velocity[:], sc.bodies[0].angular_velocity)
+    assert np.array_equal(body.angular_velocity[:], sc.bodies[0].angular_velocity)
+    np.testing.assert_allclose(gb.orientation[:], body.orientation[:], atol=1e-6)
+    assert np.abs(np.array(spun.angular_velocity[:])).max() > 1e-3
+    assert max_err_dx(b.get_particles(0)["position"], c.get_particles()["position"], sc.dx) < POS_TOL_100
