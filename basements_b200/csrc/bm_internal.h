@@ -313,7 +313,11 @@ void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int6
 // upper bound of its candidate blocks, e.g. m1_max_candidates), total CTAs.
 void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies, const int64_t* d_cand_prefix,
                     int64_t total_candidates, int cur, double* d_acc, cudaStream_t st);
-void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st);
+// The FP64 sums of n_bodies bodies -> reactions in d_out; the sums are zeroed
+// after reading (they start at zero for the next call).
+void launch_reaction_finalize(double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st);
+// One body of scene P.scene over its candidate blocks, P passed by value.
+void launch_m1_one(const SceneTable& t, const M1Params& P, int cur, double* d_acc, cudaStream_t st);
 // Loads the code of the M1 and reaction-finalize kernels on the current
 // device (a no-op once loaded).
 cudaError_t load_m1_kernels();

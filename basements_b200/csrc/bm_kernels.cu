@@ -29,6 +29,7 @@
 // B200: float atomics on shared memory are a compare-and-swap loop, and the
 // per-bin barriers stalled the warps.)
 #include <algorithm>
+#include <cfloat>
 
 #include "bm_internal.h"
 #include "bm_math.cuh"
@@ -400,10 +401,10 @@ __global__ void __launch_bounds__(kParticleCTA) k_g2p(SceneTable t, int cur, int
 // multiplies instead of skipping, which is the same for finite grid values.
 __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, int64_t EYZ, int64_t EZ,
                                               const float wgt[3][3], const float dcs[3][3], float v[3],
-                                              float Cm[9], uint32_t& heavy) {
+                                              float Cm[9], float& min_mass) {
     // separable in k: per (i, j) row, s = sum_k w_k v_k and t = sum_k w_k dk v_k,
-    // then v += w_ij s and C += w_ij (di s, dj s, t); bit 9i+3j+k of heavy is
-    // set when that node's particle mass is at least kHeavyNodeMass
+    // then v += w_ij s and C += w_ij (di s, dj s, t); min_mass is the least
+    // particle mass of the 27 nodes
     const float wd2[3] = {wgt[2][0] * dcs[2][0], wgt[2][1] * dcs[2][1], wgt[2][2] * dcs[2][2]};
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -411,8 +412,7 @@ __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, in
         for (int j = 0; j < 3; ++j) {
             const float4* row = src + i * EYZ + j * EZ;
             const float4 n[3] = {row[0], row[1], row[2]};
-#pragma unroll
-            for (int k = 0; k < 3; ++k) heavy |= (n[k].w >= kHeavyNodeMass ? 1u : 0u) << (9 * i + 3 * j + k);
+            min_mass = fminf(min_mass, fminf(n[0].w, fminf(n[1].w, n[2].w)));
             const float sx = (n[0].x * wgt[2][0] + n[1].x * wgt[2][1]) + n[2].x * wgt[2][2];
             const float sy = (n[0].y * wgt[2][0] + n[1].y * wgt[2][1]) + n[2].y * wgt[2][2];
             const float sz = (n[0].z * wgt[2][0] + n[1].z * wgt[2][1]) + n[2].z * wgt[2][2];
@@ -432,14 +432,22 @@ __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, in
         }
 }
 
-// mark_stencil_blocks for particles in base-node order: a lane whose block
-// range equals that of the lane before it leaves the marks to that lane, and
-// the allocated flags are skipped when alloc_done (the blocks of a stencil the
-// particle gathered from in full were allocated by its own scatter, or the
-// lane that covered it, one step earlier).
+// mark_stencil_blocks for particles in base-node order, per warp. A full warp
+// (warp_mask all ones) takes the box of its lanes' block ranges (redux
+// min/max per axis); when that box, each extent rounded up to a power of two,
+// holds at most 32 blocks, each lane takes one block of it (its lane index
+// split into the three coordinates by shifts) and marks it if some lane's
+// range covers it: a per-axis
+// ballot gives the lanes covering each block coordinate, and a block is
+// covered by the lanes in all three. Otherwise (a partial warp, a wide box,
+// a lane far outside) a lane whose block range equals that of the lane
+// before it leaves the marks to that lane. The allocated flags are skipped
+// for blocks whose covering lanes all have alloc_done (the blocks of a
+// stencil the particle gathered from in full were allocated by its own
+// scatter, or the lane that covered it, one step earlier).
 __device__ __forceinline__ void mark_stencil_blocks_warp(const GridDesc& g, const GridAcc& a, uint8_t* alloc,
                                                          const int base[3], const float wx[3], const float wy[3],
-                                                         const float wz[3], bool alloc_done) {
+                                                         const float wz[3], bool alloc_done, unsigned warp_mask) {
     const int lo0 = base[0] + (wx[0] == 0.0f), hi0 = base[0] + 2 - (wx[2] == 0.0f);
     const int lo1 = base[1] + (wy[0] == 0.0f), hi1 = base[1] + 2 - (wy[2] == 0.0f);
     const int lo2 = base[2] + (wz[0] == 0.0f), hi2 = base[2] + 2 - (wz[2] == 0.0f);
@@ -447,10 +455,45 @@ __device__ __forceinline__ void mark_stencil_blocks_warp(const GridDesc& g, cons
     const int e0 = ((hi0 - g.ox) >> 2) - b0, e1 = ((hi1 - g.oy) >> 2) - b1, e2 = ((hi2 - g.oz) >> 2) - b2;
     const int lane = (int)(threadIdx.x & 31);
     // a 3-node stencil covers one or two blocks per axis (e in {0, 1}); block
-    // indices far outside the box (a non-finite position) get a key of their
-    // own so that they never stand in for another lane
+    // indices far outside the box come from a non-finite position
     const bool near_box = (unsigned)(b0 + 1) <= (unsigned)(g.nbx + 1) && (unsigned)(b1 + 1) <= (unsigned)(g.nby + 1) &&
                           (unsigned)(b2 + 1) <= (unsigned)(g.nbz + 1);
+    if (warp_mask == 0xffffffffu && __all_sync(warp_mask, near_box)) {
+        const int m0 = __reduce_min_sync(warp_mask, b0), m1 = __reduce_min_sync(warp_mask, b1),
+                  m2 = __reduce_min_sync(warp_mask, b2);
+        const int x0 = __reduce_max_sync(warp_mask, b0 + e0) - m0 + 1,
+                  x1 = __reduce_max_sync(warp_mask, b1 + e1) - m1 + 1,
+                  x2 = __reduce_max_sync(warp_mask, b2 + e2) - m2 + 1;
+        // log2 of each extent rounded up to a power of two
+        const int l0 = x0 > 1 ? 32 - __clz(x0 - 1) : 0, l1 = x1 > 1 ? 32 - __clz(x1 - 1) : 0,
+                  l2 = x2 > 1 ? 32 - __clz(x2 - 1) : 0;
+        if (l0 + l1 + l2 <= 5) {
+            const int c2 = lane & ((1 << l2) - 1), c1 = (lane >> l2) & ((1 << l1) - 1), c0 = lane >> (l1 + l2);
+            unsigned cov0 = 0u, cov1 = 0u, cov2 = 0u;
+            for (int v = 0; v < x0; ++v) {
+                const unsigned bal = __ballot_sync(warp_mask, b0 <= m0 + v && m0 + v <= b0 + e0);
+                if (v == c0) cov0 = bal;
+            }
+            for (int v = 0; v < x1; ++v) {
+                const unsigned bal = __ballot_sync(warp_mask, b1 <= m1 + v && m1 + v <= b1 + e1);
+                if (v == c1) cov1 = bal;
+            }
+            for (int v = 0; v < x2; ++v) {
+                const unsigned bal = __ballot_sync(warp_mask, b2 <= m2 + v && m2 + v <= b2 + e2);
+                if (v == c2) cov2 = bal;
+            }
+            const unsigned need_alloc = __ballot_sync(warp_mask, !alloc_done);
+            const unsigned cov = cov0 & cov1 & cov2;
+            const int i = m0 + c0, j = m1 + c1, k = m2 + c2;
+            if (c0 < x0 && c1 < x1 && c2 < x2 && cov != 0u && (unsigned)i < (unsigned)g.nbx && (unsigned)j < (unsigned)g.nby &&
+                (unsigned)k < (unsigned)g.nbz) {
+                const int64_t blk = g.block_of(i, j, k);
+                if ((cov & need_alloc) != 0u && alloc[blk] == 0) alloc[blk] = 1;
+                touch_block(a, blk);
+            }
+            return;
+        }
+    }
     const unsigned long long key = near_box ? ((unsigned long long)(b0 & 0xFFFFF) << 43) |
                                                   ((unsigned long long)(b1 & 0xFFFFF) << 23) |
                                                   ((unsigned long long)(b2 & 0xFFFFF) << 3) |
@@ -490,6 +533,9 @@ __device__ __forceinline__ void mark_stencil_blocks_warp(const GridDesc& g, cons
 // separately).
 template <bool Fast>
 __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
+    // the lanes of this warp that hold a particle (the others returned before
+    // the call); every one of them reaches the block marking at the end
+    const unsigned warp_mask = __activemask();
     const GridDesc& g = S.g;
     const FusedScene& ps = S;
     int dropped = 0;
@@ -515,7 +561,7 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
     float Cm[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) Cm[q] = 0.0f;
-    uint32_t heavy = 0u;
+    float min_mass = 0.0f;  // least particle mass of the gathered stencil's nodes (0: not gathered in full)
     const int gbase0 = base[0], gbase1 = base[1], gbase2 = base[2];
     // no end weight exactly 0: the gather stencil spans all of base..base+2
     const bool gather_full = wgt[0][0] != 0.0f && wgt[0][2] != 0.0f && wgt[1][0] != 0.0f && wgt[1][2] != 0.0f &&
@@ -533,7 +579,8 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
             for (int a = 0; a < 3; ++a)
 #pragma unroll
                 for (int i = 0; i < 3; ++i) dcs[a][i] = dd[a][i] * cs;
-            gather_inside(cur_mv + g.node_rel(r0, r1, r2), EYZ, EZ, wgt, dcs, v, Cm, heavy);
+            min_mass = FLT_MAX;
+            gather_inside(cur_mv + g.node_rel(r0, r1, r2), EYZ, EZ, wgt, dcs, v, Cm, min_mass);
         } else {
 #pragma unroll 1
             for (int n = 0; n < 27; ++n) {
@@ -609,7 +656,9 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
         for (int i = 0; i < 3; ++i) dd[a][i] = ((float)(base[a] + i) - fx[a] - 0.5f) * g.dx;
     }
     const bool same_base = base[0] == gbase0 && base[1] == gbase1 && base[2] == gbase2;
-    if (!same_base) heavy = 0u;
+    // every node of the stencil was heavy in the gathered grid: no light
+    // contribution of this particle needs its force record (the bulk case)
+    const bool all_heavy = same_base && min_mass >= kHeavyNodeMass;
     {
         const int r0 = base[0] - g.ox, r1 = base[1] - g.oy, r2 = base[2] - g.oz;
         const bool inside = (unsigned)r0 <= (unsigned)(g.ex() - 3) && (unsigned)r1 <= (unsigned)(g.ey() - 3) &&
@@ -619,7 +668,6 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
         if (inside) {
             float4* dmv = next.mv + g.node_rel(r0, r1, r2);
             float4* df = next.f + g.node_rel(r0, r1, r2);
-            uint32_t light = 0u;  // bit 9i+3j+k: w m <= 1e-6 at that node
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 // m v + (m C + dt S) d, summed axis by axis
@@ -639,26 +687,30 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
                         const int64_t off = i * EYZ + j * EZ + k;
                         red_v4(dmv + off, (uj[0] + Mq[2] * dd[2][k]) * w, (uj[1] + Mq[5] * dd[2][k]) * w,
                                (uj[2] + Mq[8] * dd[2][k]) * w, mc);
-                        if (mc <= 1e-6f) light |= 1u << (9 * i + 3 * j + k);
                     }
                 }
             }
-            // the force records of light contributions at nodes that were not
-            // heavy, off the unrolled loop (few per particle)
-            light &= ~heavy;
+            // the force records of light contributions (w m <= 1e-6, the same
+            // product as the mass lane above) at nodes that were not heavy in
+            // the gathered grid, off the unrolled loop: only particles at the
+            // fringe of the material get here
+            if (!all_heavy) {
+                const float4* __restrict__ gathered = S.cur_mv + g.node_rel(r0, r1, r2);
 #pragma unroll 1
-            while (light) {
-                const int n = __ffs(light) - 1;
-                light &= light - 1;
-                const int i = n / 9, j = (n / 3) % 3, k = n % 3;
-                const float w = pick3(wgt[0], i) * pick3(wgt[1], j) * pick3(wgt[2], k);
-                const float d0 = pick3(dd[0], i), d1 = pick3(dd[1], j), d2 = pick3(dd[2], k);
-                float S_[9];
+                for (int n = 0; n < 27; ++n) {
+                    const int i = n / 9, j = (n / 3) % 3, k = n % 3;
+                    const float w = pick3(wgt[0], i) * pick3(wgt[1], j) * pick3(wgt[2], k);
+                    if (w == 0.0f || !(w * m <= 1e-6f)) continue;
+                    const int64_t off = i * EYZ + j * EZ + k;
+                    if (same_base && gathered[off].w >= kHeavyNodeMass) continue;
+                    const float d0 = pick3(dd[0], i), d1 = pick3(dd[1], j), d2 = pick3(dd[2], k);
+                    float S_[9];
 #pragma unroll
-                for (int q = 0; q < 9; ++q) S_[q] = sk_park[q * kMaxFusedThreads + threadIdx.x];
-                red_v4(df + (i * EYZ + j * EZ + k), ((S_[0] * d0 + S_[1] * d1) + S_[2] * d2) * w,
-                       ((S_[3] * d0 + S_[4] * d1) + S_[5] * d2) * w, ((S_[6] * d0 + S_[7] * d1) + S_[8] * d2) * w,
-                       0.0f);
+                    for (int q = 0; q < 9; ++q) S_[q] = sk_park[q * kMaxFusedThreads + threadIdx.x];
+                    red_v4(df + off, ((S_[0] * d0 + S_[1] * d1) + S_[2] * d2) * w,
+                           ((S_[3] * d0 + S_[4] * d1) + S_[5] * d2) * w,
+                           ((S_[6] * d0 + S_[7] * d1) + S_[8] * d2) * w, 0.0f);
+                }
             }
         } else {
 #pragma unroll 1
@@ -684,7 +736,8 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
             }
         }
     }
-    mark_stencil_blocks_warp(g, S.next, S.alloc, base, wgt[0], wgt[1], wgt[2], same_base && gather_full);
+    __syncwarp(warp_mask);
+    mark_stencil_blocks_warp(g, S.next, S.alloc, base, wgt[0], wgt[1], wgt[2], same_base && gather_full, warp_mask);
     if (!fin) atomicOr(S.status, ERR_NONFINITE);
     if (dropped) {
         atomicOr(S.status, ERR_ESCAPE);

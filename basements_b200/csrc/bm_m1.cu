@@ -396,28 +396,16 @@ __global__ void __launch_bounds__(64) k_m45(SceneTable t, const M1Params* params
 // cand_prefix NULL: grid (max candidates, bodies), body = blockIdx.y.
 // Otherwise a flat grid over the bodies' candidate bounds: body b owns CTAs
 // [cand_prefix[b], cand_prefix[b+1]).
-__global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params, int cur, double* acc_all,
-                                           const int64_t* __restrict__ cand_prefix, int n_bodies) {
-    int body = blockIdx.y;
-    int64_t cb = blockIdx.x;
-    if (cand_prefix) {
-        int lo = 0, hi = n_bodies - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (cand_prefix[mid] <= (int64_t)blockIdx.x) lo = mid;
-            else hi = mid - 1;
-        }
-        body = lo;
-        cb = (int64_t)blockIdx.x - cand_prefix[lo];
-    }
-    const M1Params& P = params[body];
+// Candidate block cb of body P (one CTA of 64 threads, one node each); the
+// CTA's reaction is added to acc (7 doubles).
+__device__ __forceinline__ void m1_candidate_block(const SceneTable& t, const M1Params& P, int64_t cb, int cur,
+                                                   double* acc) {
     if (!P.active) return;
     const int64_t ncand = (int64_t)P.nbi * P.nbj * P.nbk;
     if (cb >= ncand) return;
     const SceneDev& S = t.scenes[P.scene];
     const GridDesc g = S.g;
     const GridAcc A = S.acc[cur];
-    double* acc = acc_all + 7 * body;
     const int bk = P.bk0 + (int)(cb % P.nbk);
     const int bj = P.bj0 + (int)((cb / P.nbk) % P.nbj);
     const int bi = P.bi0 + (int)(cb / ((int64_t)P.nbk * P.nbj));
@@ -485,10 +473,35 @@ __global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params,
     }
 }
 
-__global__ void k_reaction_finalize(const double* acc, int n, bm_reaction_t* out) {
+__global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params, int cur, double* acc_all,
+                                           const int64_t* __restrict__ cand_prefix, int n_bodies) {
+    int body = blockIdx.y;
+    int64_t cb = blockIdx.x;
+    if (cand_prefix) {
+        int lo = 0, hi = n_bodies - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cand_prefix[mid] <= (int64_t)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        body = lo;
+        cb = (int64_t)blockIdx.x - cand_prefix[lo];
+    }
+    m1_candidate_block(t, params[body], cb, cur, acc_all + 7 * body);
+}
+
+// One body, its parameters passed by value (no upload before the launch).
+__global__ void __launch_bounds__(64) k_m1_one(SceneTable t, const __grid_constant__ M1Params P, int cur,
+                                               double* acc) {
+    m1_candidate_block(t, P, blockIdx.x, cur, acc);
+}
+
+// The reactions from the FP64 sums, which are zeroed after reading so that
+// the next call's sums start from zero.
+__global__ void k_reaction_finalize(double* acc, int n, bm_reaction_t* out) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= n) return;
-    const double* a = acc + 7 * b;
+    double* a = acc + 7 * b;
     bm_reaction_t r;
     for (int q = 0; q < 3; ++q) {
         r.force[q] = (float)a[q];
@@ -496,6 +509,7 @@ __global__ void k_reaction_finalize(const double* acc, int n, bm_reaction_t* out
     }
     r.nodes_inside = (int32_t)a[6];
     out[b] = r;
+    for (int q = 0; q < 7; ++q) a[q] = 0.0;
 }
 
 __global__ void k_body_prepare(SceneTable t, const BodyDev* bodies, int n, M1Params* params) {
@@ -634,6 +648,12 @@ void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int6
                                                                              n_bodies);
 }
 
+void launch_m1_one(const SceneTable& t, const M1Params& P, int cur, double* d_acc, cudaStream_t st) {
+    const int64_t cand = (int64_t)P.nbi * P.nbj * P.nbk;
+    if (!P.active || cand <= 0) return;
+    k_m1_one<<<(unsigned)cand, 64, 0, st>>>(t, P, cur, d_acc);
+}
+
 void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies, const int64_t* d_cand_prefix,
                     int64_t total_candidates, int cur, double* d_acc, cudaStream_t st) {
     if (n_bodies <= 0 || total_candidates <= 0) return;
@@ -649,7 +669,7 @@ cudaError_t load_m1_kernels() {
     return e;
 }
 
-void launch_reaction_finalize(const double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st) {
+void launch_reaction_finalize(double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st) {
     if (n_bodies <= 0) return;
     k_reaction_finalize<<<nblk(n_bodies, 64), 64, 0, st>>>(d_acc, n_bodies, d_out);
 }

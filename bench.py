@@ -208,8 +208,6 @@ def run_ours(args, ranks: Ranks):
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
     idx = ranks.local if ranks.world > 1 else 0
     sampler = ClockSampler(vis[idx] if idx < len(vis) and vis[idx] else str(idx))
-    s.profile(True)
-    s.profile_reset()
     s.sync()
     suspects0 = s.light_node_suspects()
     ranks.barrier()
@@ -220,7 +218,6 @@ def run_ours(args, ranks: Ranks):
     ms = s.timer_stop()
     clocks = sampler.stop()
     ranks.barrier()
-    prof = s.profile_read()
     st, esc = s.sync()
     if st != 0:
         raise RuntimeError(f"timed steps reported status {st} ({esc} escaped writes)")
@@ -228,6 +225,22 @@ def run_ours(args, ranks: Ranks):
     ms_max = ranks.max(ms)
     per_step_ms = ms_max / args.steps
     value = sc.n * args.steps * ranks.world / (ms_max / 1e3)
+    # per-kernel times: the same number of steps again, each phase between two
+    # CUDA events on the solver stream (the events add gaps of their own, so
+    # this pass is not the timed one)
+    s.profile(True)
+    s.profile_reset()
+    step1 = step0 + args.steps
+    s.timer_start()
+    for i in range(args.steps):
+        s.step_coupled(sc.dt, [collider(step1 + i)], read_reactions=False)
+    ms_profiled = s.timer_stop()
+    prof = s.profile_read()
+    s.profile(False)
+    st, esc = s.sync()
+    if st != 0:
+        raise RuntimeError(f"profiled steps reported status {st} ({esc} escaped writes)")
+    suspects = s.light_node_suspects() - suspects0  # over both passes
 
     # roofline of the dominant kernel
     bpu = bytes_per_unit(sc.n, touched)
@@ -241,6 +254,7 @@ def run_ours(args, ranks: Ranks):
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get(dom)
+    kernel_ms_per_step = sum(v[0] for v in kernels.values()) / args.steps
     launches = sum(v[1] for k, v in kernels.items() if k != "grid_clear")
     launches += 2 * kernels.get("bin_sort", (0, 0))[1]  # key + scan + permute per sort
     # a folded grid update is the update plus the three light-node repair
@@ -262,11 +276,17 @@ def run_ours(args, ranks: Ranks):
                      "step_achieved_gbs": step_roof_gbs, "step_frac": step_roof_gbs / peak,
                      "bytes_per_particle_step": bpu["step"] / sc.n},
         "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in kernels.items()},
+        # where a step's time goes: the sum of the phases' event-timed
+        # durations per step (profiled pass) against the unprofiled step; the
+        # rest is the gaps between launches and small copies
+        "step_breakdown_ms": {"step": per_step_ms, "phases_sum": kernel_ms_per_step,
+                              "gaps": per_step_ms - kernel_ms_per_step,
+                              "step_profiled": ms_profiled / args.steps},
         "clocks": clocks,
         "gpu_launches": int(launches),
-        # nodes of the timed steps where the fused kernel's light-node rule
-        # could have missed a force record; each such step's grid was redone
-        # unfolded on the device (exact)
+        # nodes of the timed and profiled steps where the fused kernel's
+        # light-node rule could have missed a force record; each such step's
+        # grid was redone unfolded on the device (exact)
         "light_node_suspects": int(suspects),
     }
     s.close()
@@ -418,7 +438,20 @@ def run_batched(args):
                            "seconds": loop_secs,
                            "what": "same scenes one after another through bm_solver_step_coupled, reaction "
                                    "read back and the body integrated on the host every step (host clock)"},
-            "speedup_vs_plain_loop": value / loop_rate}
+            "speedup_vs_plain_loop": value / loop_rate,
+            "cpu_baseline": _aggregate_or_none(args, "box_drop", list(range(len(scs))))}
+
+
+def _aggregate_or_none(args, gen, seeds):
+    if args.no_cpu_baseline:
+        return None
+    from oracle import oracle as O
+    kind = O.reference_or_port()
+    if not O.available(kind):
+        return None
+    # one scene per core, at most 64 processes (a few hundred MB each)
+    cores = min(os.cpu_count() or 1, 64)
+    return cpu_aggregate(gen, seeds[:cores], kind)
 
 
 def run_served(args):
@@ -489,7 +522,8 @@ def run_served(args):
                            "seconds": loop_secs,
                            "what": "the first rate's requests one after another through the drop-in solver "
                                    "(host clock, body integrated on the host every step)"},
-            "speedup_vs_plain_loop": best / loop_rate}
+            "speedup_vs_plain_loop": best / loop_rate,
+            "cpu_baseline": _aggregate_or_none(args, "serve", list(range(args.serve_requests)))}
 
 
 def run_adjoint(args):
@@ -536,6 +570,73 @@ def run_adjoint(args):
             "gradient_check": "tests/test_gpu_adjoint.py (FP64 central differences)"}
 
 
+def host_cpu():
+    """The host's logical core count and CPU model (from /proc/cpuinfo)."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
+def _cpu_scene_worker(job):
+    """One process of the aggregate CPU baseline: the reference's own solver
+    (coupler and integrator included) on one scene for `steps` steps, as the
+    reference's harness runs a scene (bench_compare_all.cpp:104-116)."""
+    kind, gen, seed, steps = job
+    from basements_b200 import scenes
+    from oracle import oracle as O
+
+    sc = scenes.box_drop_scene(seed) if gen == "box_drop" else scenes.serve_request_scene(seed)
+    c = O.CpuSolver(kind, sc.dx)
+    c.set_material(sc.E, sc.nu, sc.rho)
+    c.set_plastic_alpha(sc.alpha)
+    c.set_gravity(sc.gravity)
+    c.set_floor_friction(sc.floor_friction)
+    c.add_particles(sc.position, None, sc.mass)
+    t0 = time.perf_counter()
+    if sc.bodies:
+        c.run_dynamic_body(O.collider(**sc.bodies[0].as_tuple()), sc.gravity, sc.dt, steps)
+    else:
+        c.step(sc.dt, steps)
+    el = time.perf_counter() - t0
+    c.close()
+    return sc.n * steps, el, sc.n
+
+
+def cpu_aggregate(gen: str, seeds, kind: str, work_per_scene: float = 8e6):
+    """Aggregate CPU baseline of a many-scene workload: the reference's solver
+    in one process per host core (spawned, so that no process inherits a CUDA
+    context), each on one scene of the sample for about work_per_scene
+    particle-steps. Returns particle-steps of all processes / wall time of the
+    whole pool."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    from basements_b200 import scenes
+
+    make = scenes.box_drop_scene if gen == "box_drop" else scenes.serve_request_scene
+    jobs = []
+    for seed in seeds:
+        n = make(seed).n
+        jobs.append((kind, gen, seed, max(1, int(round(work_per_scene / max(n, 1))))))
+    procs = min(os.cpu_count() or 1, len(jobs))
+    t0 = time.perf_counter()
+    with cf.ProcessPoolExecutor(max_workers=procs, mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_cpu_scene_worker, jobs))
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    return {"value": work / wall, "unit": UNIT, "cores": procs,
+            "kind": "reference" if kind == "ref" else "port",
+            "sample": f"{len(jobs)} scenes of the workload ({gen} seeds {seeds[0]}..{seeds[-1]}), one process "
+                      f"per core, ~{work_per_scene:.0e} particle-steps each ({wall:.1f} s wall)",
+            "host": host_cpu()}
+
+
 def cpu_reference_rate(sc, n_steps: int, kind: str):
     """Times the reference's own CPU MPMSolver (oracle/_ref, else the pinned
     float restatement) on the wheel-rut scene: P2G, update_grid, M1 apply,
@@ -573,7 +674,7 @@ def run_reference(args, ranks: Ranks):
     rate, el = cpu_reference_rate(sc, n_timed, kind)
     sample = f"{n_timed} coupled steps of the {sc.n}-particle wheel-rut scene"
     cb = {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference" if kind == "ref" else "port",
-          "sample": sample}
+          "sample": sample, "host": host_cpu()}
     return {"metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": ranks.world,
             "steps": n_timed, "warmup": n_warm, "ms_per_step": el * 1e3 / n_timed, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded wheel-rut sand bed)",
@@ -610,7 +711,8 @@ def main():
                 out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1,
                                        "kind": "reference" if kind == "ref" else "port",
                                        "sample": f"3 coupled steps of the {sc.n}-particle wheel-rut scene "
-                                                 f"({el:.1f} s, 1 thread)"}
+                                                 f"({el:.1f} s, 1 thread: the reference is single-threaded)",
+                                       "host": host_cpu()}
         if ranks.rank == 0:
             print(json.dumps(out), flush=True)
     finally:

@@ -121,22 +121,66 @@ template <class R> struct M3 {
     }
 };
 
+// Record of the discontinuous decisions of a run, for the finite-difference
+// checks of the adjoint: a central difference is only a derivative of the
+// run if its two sides take the same decisions. Covered: the SVD's pair skip
+// (|a_ij| < 1e-6) and sweep stop (below 1e-5), and the coupler's inside test
+// per node; each is folded into a hash in the order the run makes them (FNV-1a
+// steps), with counts beside.
+// A DecisionTape holds the decisions themselves, so that a run can record
+// them and another run replay them: the two sides of a central difference
+// then follow the same branch, and their difference is a derivative of that
+// branch. One 16-bit code per SVD call (the skip bit of each pair in the
+// order visited; the number of sweeps in bits 12-14, or bit 15 for all five
+// sweeps with the 15 skip bits below), and per coupler call the sorted keys of
+// the nodes inside.
+struct DecisionTape {
+    std::vector<uint16_t> svd;
+    std::vector<std::vector<int64_t>> inside;
+    size_t svd_pos = 0, inside_pos = 0;
+    bool replay = false;
+    bool overrun = false;  // a replay asked for more decisions than recorded
+};
+
+struct DecisionLog {
+    uint64_t svd_hash = 14695981039346656037ull, inside_hash = 14695981039346656037ull;
+    int64_t rotations = 0, sweeps = 0, inside = 0;
+    DecisionTape* tape = nullptr;
+    static void mix(uint64_t& h, uint64_t v) { h = (h ^ v) * 1099511628211ull; }
+};
+
 // svd.h:18-108. Cyclic Jacobi eigen-solve of A = F^T F: at most 5 sweeps over
 // the pairs (0,1),(0,2),(1,2); a pair is skipped when |a_ij| < 1e-6; the sweep
 // loop stops once the largest off-diagonal seen in a sweep is below 1e-5.
 // sigma_k = sqrt(max(0, A_kk)), U_k = (F V)_k / sigma_k or the unit axis when
 // sigma_k <= 1e-6. Singular values are left unsorted, no determinant fix.
 template <class R>
-void svd3(const M3<R>& F, M3<R>& U, V3<R>& S, M3<R>& V) {
+void svd3(const M3<R>& F, M3<R>& U, V3<R>& S, M3<R>& V, DecisionLog* L = nullptr) {
     M3<R> A = F.T() * F;
     V = M3<R>::identity();
+    DecisionTape* T = L ? L->tape : nullptr;
+    uint16_t code = 0;
+    int rep_sweeps = 0;
+    if (T && T->replay) {
+        if (T->svd_pos < T->svd.size()) code = T->svd[T->svd_pos++];
+        else T->overrun = true;
+        rep_sweeps = (code & 0x8000u) ? 5 : ((code >> 12) & 7);
+    }
+    int bit = 0, done = 0;
     for (int sweep = 0; sweep < 5; ++sweep) {
         R max_off = 0;
         for (int i = 0; i < 2; ++i) {
             for (int j = i + 1; j < 3; ++j) {
                 const R a_ij = A.m[i][j], a_ii = A.m[i][i], a_jj = A.m[j][j];
                 max_off = std::max(max_off, std::abs(a_ij));
-                if (std::abs(a_ij) < R(1e-6f)) continue;
+                const bool skip = (T && T->replay) ? ((code >> bit) & 1u) != 0 : std::abs(a_ij) < R(1e-6f);
+                if (T && !T->replay && skip) code |= (uint16_t)(1u << bit);
+                ++bit;
+                if (L) {
+                    DecisionLog::mix(L->svd_hash, skip ? 1u : 2u);
+                    L->rotations += skip ? 0 : 1;
+                }
+                if (skip) continue;
                 const R tau = (a_jj - a_ii) / (R(2) * a_ij);
                 R t;
                 if (tau >= R(0)) t = R(1) / (tau + std::sqrt(R(1) + tau * tau));
@@ -160,7 +204,18 @@ void svd3(const M3<R>& F, M3<R>& U, V3<R>& S, M3<R>& V) {
                 }
             }
         }
-        if (max_off < R(1e-5f)) break;
+        const bool stop = (T && T->replay) ? sweep + 1 == rep_sweeps : max_off < R(1e-5f);
+        if (L) {
+            DecisionLog::mix(L->svd_hash, stop ? 3u : 4u);
+            L->sweeps += 1;
+        }
+        done = sweep + 1;
+        if (stop) break;
+    }
+    if (T && !T->replay) {
+        if (done == 5) code |= 0x8000u;
+        else code |= (uint16_t)(done << 12);
+        T->svd.push_back(code);
     }
     const R s0 = std::sqrt(std::max(R(0), A.m[0][0]));
     const R s1 = std::sqrt(std::max(R(0), A.m[1][1]));
@@ -247,6 +302,8 @@ public:
     V3<R> gravity{R(0), R(-9.81f), R(0)};
     R alpha = R(0.40f), E = R(1.0e5f), nu = R(0.3f), density = R(1500.0f);
     R floor_friction = R(0.4f);
+    DecisionLog* log = nullptr;  // records the SVD decisions of the steps when set
+    DecisionLog log_store;
 
     void initialize(R dx) { grid = Grid<R>(dx); }
     R mu_lame() const { return E / (R(2) * (R(1) + nu)); }
@@ -290,7 +347,7 @@ public:
         const M3<R> Ft = (M3<R>::identity() + p.C * dt) * p.F;
         M3<R> U, V;
         V3<R> sig;
-        svd3(Ft, U, sig, V);
+        svd3(Ft, U, sig, V, log);
         sig.x = std::max(sig.x, R(1e-6f));
         sig.y = std::max(sig.y, R(1e-6f));
         sig.z = std::max(sig.z, R(1e-6f));
@@ -326,7 +383,7 @@ public:
 
         M3<R> U, V;
         V3<R> sg;
-        svd3(p.F, U, sg, V);
+        svd3(p.F, U, sg, V, log);
         sg.x = std::max(sg.x, R(1e-6f));
         sg.y = std::max(sg.y, R(1e-6f));
         sg.z = std::max(sg.z, R(1e-6f));
@@ -427,7 +484,7 @@ template <class R> bool shape_inside(const ColliderF& b, const V3<R>& l) {
 // whose node-centre span overlaps the box-formula AABB; nodes inside the shape
 // take the mass-weighted average of node and body velocity and gain m_b; the
 // reaction sums m_b (v_after - v_body) / dt and its moment about the centre.
-template <class R> Reaction<R> m1_apply(Grid<R>& grid, const ColliderF& b, R dt) {
+template <class R> Reaction<R> m1_apply(Grid<R>& grid, const ColliderF& b, R dt, DecisionLog* L = nullptr) {
     Reaction<R> out;
     if (dt <= R(0)) return out;
     const R dx = grid.dx;
@@ -444,6 +501,15 @@ template <class R> Reaction<R> m1_apply(Grid<R>& grid, const ColliderF& b, R dt)
     const V3<R> lo = c - ah, hi = c + ah;
     const V3<R> vl(b.linear_velocity[0], b.linear_velocity[1], b.linear_velocity[2]);
     const V3<R> w(b.angular_velocity[0], b.angular_velocity[1], b.angular_velocity[2]);
+    // decision tape: the nodes found inside (recording) or to treat as inside
+    // (replay) in this call
+    std::vector<int64_t> rec_in;
+    static const std::vector<int64_t> kNone;
+    const std::vector<int64_t>* rep_in = &kNone;
+    if (L && L->tape && L->tape->replay) {
+        if (L->tape->inside_pos < L->tape->inside.size()) rep_in = &L->tape->inside[L->tape->inside_pos++];
+        else L->tape->overrun = true;
+    }
     V3<R> fsum, tsum;
     for (auto& kv : grid.blocks) {
         Block<R>& blk = kv.second;
@@ -460,7 +526,19 @@ template <class R> Reaction<R> m1_apply(Grid<R>& grid, const ColliderF& b, R dt)
                     const V3<R> xn(((R)(blk.ox + li) + R(0.5f)) * dx, ((R)(blk.oy + lj) + R(0.5f)) * dx,
                                    ((R)(blk.oz + lk) + R(0.5f)) * dx);
                     const V3<R> local = Rw2l * (xn - c);
-                    if (!shape_inside<R>(b, local)) continue;
+                    bool in = shape_inside<R>(b, local);
+                    if (L && L->tape) {
+                        const int64_t key = ((int64_t)(blk.ox + li + (1 << 20)) << 42) |
+                                            ((int64_t)(blk.oy + lj + (1 << 20)) << 21) |
+                                            (int64_t)(blk.oz + lk + (1 << 20));
+                        if (L->tape->replay) in = std::binary_search(rep_in->begin(), rep_in->end(), key);
+                        else if (in) rec_in.push_back(key);
+                    }
+                    if (L) {
+                        DecisionLog::mix(L->inside_hash, in ? 5u : 6u);
+                        L->inside += in ? 1 : 0;
+                    }
+                    if (!in) continue;
                     const V3<R> r = xn - c;
                     const V3<R> vb = vl + w.cross(r);
                     V3<R> va;
@@ -478,6 +556,10 @@ template <class R> Reaction<R> m1_apply(Grid<R>& grid, const ColliderF& b, R dt)
                     tsum += r.cross(dF);
                     ++out.nodes_inside;
                 }
+    }
+    if (L && L->tape && !L->tape->replay) {
+        std::sort(rec_in.begin(), rec_in.end());
+        L->tape->inside.push_back(std::move(rec_in));
     }
     out.force = fsum;
     out.torque = tsum;

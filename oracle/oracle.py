@@ -103,6 +103,13 @@ def load(kind: str):
         "run_dynamic_body": fn("run_dynamic_body", None, C.c_void_p, C.POINTER(OrcCollider), C.c_float, C.c_float,
                                C.c_float, C.c_float, C.c_int, _f),
     }
+    if hasattr(lib, f"{p}_decisions_read"):
+        api["decisions_enable"] = fn("decisions_enable", None, C.c_void_p, C.c_int)
+        api["decisions_read"] = fn("decisions_read", None, C.c_void_p, C.POINTER(C.c_uint64))
+        api["tape_new"] = fn("tape_new", C.c_void_p)
+        api["tape_free"] = fn("tape_free", None, C.c_void_p)
+        api["solver_use_tape"] = fn("solver_use_tape", None, C.c_void_p, C.c_void_p, C.c_int)
+        api["tape_status"] = fn("tape_status", None, C.c_void_p, C.POINTER(C.c_int64))
     _loaded[kind] = api
     return api
 
@@ -259,6 +266,22 @@ class CpuSolver:
                                      None if ii is None else _p(ii))
         return body
 
+    def decisions(self, enable=None):
+        """Restatement only: with enable=True/False turns the record of the
+        run's discontinuous decisions on (cleared) or off; returns the record
+        so far: (svd hash, inside hash, rotations, sweeps, inside count)."""
+        if enable is not None:
+            self.api["decisions_enable"](self.h, 1 if enable else 0)
+        out = (C.c_uint64 * 5)()
+        self.api["decisions_read"](self.h, out)
+        return tuple(int(v) for v in out)
+
+    def use_tape(self, tape: "DecisionTape | None", mode: str = "off"):
+        """Restatement only: record this solver's discontinuous decisions into
+        `tape` ("record"), take them from it ("replay"), or detach ("off")."""
+        m = {"off": 0, "record": 1, "replay": 2}[mode]
+        self.api["solver_use_tape"](self.h, tape.t if tape is not None else None, m)
+
     def grid_nodes(self):
         """Every node of every allocated 4^3 block, as a dict keyed by (i,j,k)."""
         cap = int(self.api["grid_num_nodes"](self.h))
@@ -276,6 +299,33 @@ class CpuSolver:
         vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
         mass = np.ascontiguousarray(mass, np.float32).reshape(-1)
         self.api["grid_seed"](self.h, len(ijk), ijk.ctypes.data_as(_i32), _p(vel), _p(mass))
+
+
+class DecisionTape:
+    """A record of a run's SVD and coupler-inside decisions (restatement
+    only), replayed by other runs so that they follow the same branch."""
+
+    def __init__(self, kind: str):
+        self.api = load(kind)
+        self.t = self.api["tape_new"]()
+
+    def status(self):
+        """(SVD calls recorded, replayed, coupler calls recorded, replayed,
+        replay ran past the record)."""
+        out = (C.c_int64 * 4)()
+        self.api["tape_status"](self.t, out)
+        return int(out[0]), int(out[1]), int(out[2]), int(out[3]) & ((1 << 40) - 1), bool(out[3] >> 40)
+
+    def close(self):
+        if self.t:
+            self.api["tape_free"](self.t)
+            self.t = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def box_drop_m1(kind: str) -> np.ndarray:

@@ -85,6 +85,21 @@ ORC_EXPORT int ORC(box_drop_m1)(float* rows, int max_rows);
  * velocities). */
 ORC_EXPORT void ORC(run_dynamic_body)(void* h, orc_collider_t* body, float gx, float gy, float gz, float dt,
                                       int n_steps, const float* inv_inertia);
+/* Restatement only (orc_*): turns on (on != 0) or off the record of the run's
+ * discontinuous decisions (SVD pair skip and sweep stop, M1 inside test) and
+ * reads it: out = {svd hash, inside hash, rotations, sweeps, inside count},
+ * each accumulated since the record was turned on. */
+ORC_EXPORT void ORC(decisions_enable)(void* h, int on);
+ORC_EXPORT void ORC(decisions_read)(void* h, uint64_t* out5);
+/* Restatement only: a tape of those decisions. mode 1 records the solver's
+ * decisions into the tape (cleared), 2 replays them from its start (the
+ * solver takes the recorded decisions instead of its own comparisons), 0
+ * detaches it. status: {SVD calls recorded, replayed; coupler calls
+ * recorded, replayed + 2^40 if a replay ran past the record}. */
+ORC_EXPORT void* ORC(tape_new)(void);
+ORC_EXPORT void ORC(tape_free)(void* t);
+ORC_EXPORT void ORC(solver_use_tape)(void* h, void* t, int mode);
+ORC_EXPORT void ORC(tape_status)(void* t, int64_t* out4);
 /* SVD of n row-major 3x3 matrices: U (n*9), sigma (n*3), V (n*9). */
 ORC_EXPORT void ORC(svd)(int64_t n, const float* F, float* U, float* S, float* V);
 

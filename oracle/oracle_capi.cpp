@@ -126,8 +126,52 @@ ORC_EXPORT void orc_p2g(void* h, float dt) { sv(h)->p2g(dt); }
 ORC_EXPORT void orc_grid_update(void* h, float dt) { sv(h)->update_grid(dt); }
 ORC_EXPORT void orc_g2p(void* h, float dt) { sv(h)->g2p(dt); }
 
+ORC_EXPORT void orc_decisions_enable(void* h, int on) {
+    S* s = sv(h);
+    DecisionTape* keep = s->log_store.tape;
+    s->log_store = DecisionLog();
+    s->log_store.tape = keep;
+    s->log = (on || keep) ? &s->log_store : nullptr;
+}
+
+ORC_EXPORT void* orc_tape_new(void) { return new DecisionTape(); }
+ORC_EXPORT void orc_tape_free(void* t) { delete static_cast<DecisionTape*>(t); }
+ORC_EXPORT void orc_solver_use_tape(void* h, void* t, int mode) {
+    S* s = sv(h);
+    DecisionTape* T = static_cast<DecisionTape*>(t);
+    if (!T || mode == 0) {
+        s->log_store.tape = nullptr;
+        return;
+    }
+    T->replay = mode == 2;
+    T->svd_pos = T->inside_pos = 0;
+    T->overrun = false;
+    if (mode == 1) {
+        T->svd.clear();
+        T->inside.clear();
+    }
+    s->log_store.tape = T;
+    s->log = &s->log_store;
+}
+ORC_EXPORT void orc_tape_status(void* t, int64_t* out4) {
+    const DecisionTape* T = static_cast<const DecisionTape*>(t);
+    out4[0] = (int64_t)T->svd.size();
+    out4[1] = (int64_t)T->svd_pos;
+    out4[2] = (int64_t)T->inside.size();
+    out4[3] = (int64_t)T->inside_pos + (T->overrun ? (int64_t(1) << 40) : 0);
+}
+
+ORC_EXPORT void orc_decisions_read(void* h, uint64_t* out5) {
+    const DecisionLog& L = sv(h)->log_store;
+    out5[0] = L.svd_hash;
+    out5[1] = L.inside_hash;
+    out5[2] = (uint64_t)L.rotations;
+    out5[3] = (uint64_t)L.sweeps;
+    out5[4] = (uint64_t)L.inside;
+}
+
 ORC_EXPORT int orc_m1_apply(void* h, const orc_collider_t* body, float dt, float* reaction6) {
-    Reaction<R> r = m1_apply<R>(sv(h)->grid, to_collider(body), (R)dt);
+    Reaction<R> r = m1_apply<R>(sv(h)->grid, to_collider(body), (R)dt, sv(h)->log);
     reaction6[0] = (float)r.force.x; reaction6[1] = (float)r.force.y; reaction6[2] = (float)r.force.z;
     reaction6[3] = (float)r.torque.x; reaction6[4] = (float)r.torque.y; reaction6[5] = (float)r.torque.z;
     return r.nodes_inside;

@@ -3,7 +3,7 @@
 Run in a container that holds the reference tree (2nugu/basements) and the
 built reference harness (``make -C oracle``):
 
-    python tests/golden/make_golden.py [--ref-root /root/reference]
+    python tests/golden/make_golden.py --ref-root <reference tree>
 
 Every array is produced either by the reference's OWN code (oracle/_ref,
 compiled from the reference headers) or read from the reference's shipped
@@ -233,7 +233,7 @@ def constitutive():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", required=True, help="root of the reference tree (2nugu/basements)")
     a = ap.parse_args()
     if not O.available("ref"):
         sys.exit("oracle/_ref/libref_mpm.so missing: run `make -C oracle` first")
