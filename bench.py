@@ -152,6 +152,33 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def kernel_sources_hash() -> str:
+    """sha256 of the CUDA library's sources (csrc/ and include/), the key
+    under which an ncu traffic figure is recorded."""
+    import glob
+    import hashlib
+    h = hashlib.sha256()
+    files = sorted(glob.glob(os.path.join(ROOT, "basements_b200", "csrc", "*")) +
+                   glob.glob(os.path.join(ROOT, "include", "*.h")))
+    for f in files:
+        h.update(os.path.basename(f).encode())
+        h.update(open(f, "rb").read())
+    return h.hexdigest()
+
+
+def kernel_traffic(kernel: str):
+    """DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)
+    of `kernel` at this workload, from profiles/traffic.json, only when that
+    capture was made from the same library sources; otherwise None."""
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(tp):
+        return None
+    rec = json.load(open(tp))
+    if rec.get("sources_sha256") != kernel_sources_hash():
+        return None
+    return rec.get(kernel)
+
+
 def bytes_per_unit(n_particles: int, touched_nodes: int):
     """Algorithmic bytes of one step (FP32 SoA): per particle 248 B (P2G reads
     x,v,C,F,m,V0 = 26 floats; G2P reads x,F = 12 and writes x,v,C,F = 24) and
@@ -250,10 +277,7 @@ def run_ours(args, ranks: Ranks):
     peak, peak_kind = measured_peak_hbm()
     alg = bpu.get(dom)
     achieved = (alg / (dom_ms / 1e3)) / 1e9 if alg else None
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dom)
+    traffic = kernel_traffic(dom)
     kernel_ms_per_step = sum(v[0] for v in kernels.values()) / args.steps
     launches = sum(v[1] for k, v in kernels.items() if k != "grid_clear")
     launches += 2 * kernels.get("bin_sort", (0, 0))[1]  # key + scan + permute per sort
@@ -699,6 +723,13 @@ def main():
             out["batched"] = run_batched(args)
         if ranks.world == 1 and "served" in forms:
             out["served"] = run_served(args)
+            sv = out["served"]
+            # what bounds the served-over-loop ratio: the plain loop already
+            # runs the large requests near the kernel's rate, so even a server
+            # at the batched kernel's rate would be this many times the loop
+            if "batched" in out:
+                sv["fraction_of_batched_rate"] = sv["value"] / out["batched"]["value"]
+                sv["ratio_ceiling_at_batched_rate"] = out["batched"]["value"] / sv["plain_loop"]["value"]
         if ranks.world == 1 and "adjoint" in forms:
             out["adjoint"] = run_adjoint(args)
         if ranks.rank == 0 and not args.no_cpu_baseline:

@@ -38,6 +38,59 @@ def _loss_job(args):
     return scenes.heightfield_loss(oracle_run(kind, sc, body, waypoints, steps, x0), target)[0]
 
 
+def _frozen_job(args):
+    """One central difference on a fixed branch: the base run records its
+    SVD and coupler-inside decisions, the two perturbed runs replay them.
+    Returns (dL, step taken, replays consistent)."""
+    from oracle import oracle as O
+
+    sc, body, wp, steps, target, k, a, eps = args
+    tape = O.DecisionTape("f64")
+
+    def loss(w, mode):
+        c = O.CpuSolver("f64", sc.dx)
+        c.set_material(sc.E, sc.nu, sc.rho)
+        c.set_plastic_alpha(sc.alpha)
+        c.add_particles(sc.position, None, sc.mass)
+        c.use_tape(tape, mode)
+        for n in range(steps):
+            b = scenes.body_on_path(body, w, steps, sc.dt, n)
+            c.p2g(sc.dt)
+            c.grid_update(sc.dt)
+            c.m1_apply(O.collider(**b.as_tuple()), sc.dt)
+            c.g2p(sc.dt)
+        pos = c.positions_f64()
+        c.close()
+        return scenes.heightfield_loss(pos, target)[0]
+
+    loss(wp, "record")
+    hi, lo = wp.copy(), wp.copy()
+    hi[k, a] = np.float32(float(wp[k, a]) + eps)
+    lo[k, a] = np.float32(float(wp[k, a]) - eps)
+    consistent = True
+    Lh = loss(hi, "replay")
+    st = tape.status()
+    consistent = consistent and st[0] == st[1] and st[2] == st[3] and not st[4]
+    Ll = loss(lo, "replay")
+    st = tape.status()
+    consistent = consistent and st[0] == st[1] and st[2] == st[3] and not st[4]
+    tape.close()
+    return Lh - Ll, float(hi[k, a]) - float(lo[k, a]), consistent
+
+
+def fd_waypoints_frozen(p, sc, body, wp, steps, target, coords, eps=1e-6):
+    """Central differences dL/d waypoint[k, a] of the FP64 run with its
+    discontinuous decisions frozen: both sides replay the SVD pair-skip and
+    sweep-stop decisions and the coupler's inside sets of the unperturbed run
+    (oracle DecisionTape), so that the difference is a derivative of one
+    branch of the algorithm, the branch an adjoint differentiates. (Left
+    free, a 1e-6 change of one waypoint flips hundreds of SVD decisions of
+    the 262k-particle tine pass, each adding its jump / 2 eps.) Returns the
+    differences and whether every replay consumed exactly the record."""
+    res = p.map(_frozen_job, [(sc, body, wp, steps, target, k, a, eps) for k, a in coords])
+    return np.array([d / st for d, st, _ in res]), all(ok for _, _, ok in res)
+
+
 def pool(n=None):
     return mp.get_context("spawn").Pool(n or min(16, os.cpu_count() or 1))
 
