@@ -153,6 +153,24 @@ __device__ __forceinline__ int scene_of_cta(const SceneTable& t, int64_t cta) {
     return lo;
 }
 
+// True in the last CTA of the launch to reach this call (every CTA must
+// reach it): each CTA, after its own work, fences its writes and counts itself
+// on *counter; the CTA that completes the count sees the others' writes and
+// resets the counter for the next launch. Nothing waits.
+__device__ __forceinline__ bool last_cta(uint32_t* counter) {
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned total = gridDim.x * gridDim.y * gridDim.z;
+        last = atomicAdd(counter, 1u) == total - 1;
+        if (last) *counter = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
 // Marks block b as holding data in `a` (appends it to the list once).
 __device__ __forceinline__ void touch_block(const GridAcc& a, int64_t b) {
     if (a.touched[b] == 0u && atomicExch(a.touched + b, 1u) == 0u) a.list[atomicAdd(a.count, 1)] = (int32_t)b;
@@ -203,10 +221,12 @@ int64_t scan_tiles(int64_t nkeys);
 // only_fresh: skip scenes whose `fresh` flag is 0 (newly admitted scenes of
 // a running table get their first P2G while the others keep theirs).
 void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st, bool only_fresh = false);
-// Exact repair of the fused kernel's light-node rule: a World's device words
-// ([0] set by the grid update when a scene found a light-node suspect, [1] a
-// count of finished CTAs of the repair) and what the repair's standalone P2G
+// Device words of a World's grid update (kWorldWords: [0] set by the grid
+// update when a scene found a light-node suspect, [1], [2] finished-CTA
+// counts of the grid update and of the repair's update, [3] of the
+// single-body M1 launch) and what the light-node repair's standalone P2G
 // needs (the table's per-particle CTAs and the current particle store).
+constexpr int kWorldWords = 4;
 struct LightRepair {
     uint32_t* word;
     int64_t n_ctas;
@@ -215,11 +235,11 @@ struct LightRepair {
 };
 // folded: acc[cur].mv holds momentum + force * dt (the force channel only
 // holds the contributions of w*m <= 1e-6 particle-node pairs); scenes whose
-// `fresh` flag is set are always treated as unfolded. With a folded grid and
-// `repair`, a scene with a light-node suspect has this step's grid redone
-// from its particles unfolded (standalone P2G, update_grid), on the device.
+// `fresh` flag is set are always treated as unfolded. With a folded grid, a
+// scene with a light-node suspect has this step's grid redone from its
+// particles unfolded (standalone P2G, update_grid), on the device.
 void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st,
-                        const LightRepair* repair = nullptr);
+                        const LightRepair* repair);
 void launch_g2p(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st);
 // Fused G2P of this step + P2G of the next (into acc[1-cur]), in one of the
 // compiled launch shapes.
@@ -316,8 +336,12 @@ void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies,
 // The FP64 sums of n_bodies bodies -> reactions in d_out; the sums are zeroed
 // after reading (they start at zero for the next call).
 void launch_reaction_finalize(double* d_acc, int n_bodies, bm_reaction_t* d_out, cudaStream_t st);
-// One body of scene P.scene over its candidate blocks, P passed by value.
-void launch_m1_one(const SceneTable& t, const M1Params& P, int cur, double* d_acc, cudaStream_t st);
+// One body of scene P.scene over its candidate blocks, P passed by value;
+// the launch's last CTA writes the reaction to d_out and zeroes the sums
+// (counter: a zero device word). Returns false, launching nothing, when the
+// body has no candidate block (the caller finalizes then).
+bool launch_m1_one(const SceneTable& t, const M1Params& P, int cur, double* d_acc, bm_reaction_t* d_out,
+                   uint32_t* counter, cudaStream_t st);
 // Loads the code of the M1 and reaction-finalize kernels on the current
 // device (a no-op once loaded).
 cudaError_t load_m1_kernels();

@@ -216,7 +216,7 @@ __device__ __forceinline__ void update_node(const GridDesc& g, const GridAcc& c,
 // this launch). A suspect is counted (escaped[1]) and marks its scene for
 // the repair that follows (escaped[2], and repair[0] for the launch).
 __global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int cur, bool folded_all,
-                                                              uint32_t* repair) {
+                                                              uint32_t* words) {
     const SceneDev& S = t.scenes[blockIdx.y];
     const bool folded = folded_all && !S.fresh;
     const GridDesc g = S.g;
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int 
                 if (m_new > 0.0f && m_new <= 1e-6f) {
                     atomicAdd(S.escaped + 1, 1ull);
                     S.escaped[2] = 1ull;
-                    if (repair) *repair = 1u;
+                    words[0] = 1u;
                 }
             }
             o.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -245,38 +245,41 @@ __global__ void __launch_bounds__(kGridThreads) k_grid_update(SceneTable t, int 
         }
         update_node(g, c, mat, dt, folded, c.list[slot], tt);
     }
+    // the last CTA: the zeroed acc[1-cur] of every scene takes the next P2G
+    // (its list restarts), and a scene marked for the light-node repair has
+    // its acc[cur] zeroed on the listed blocks (the list and the block flags
+    // stay) for the repair's P2G
+    if (!last_cta(words + 1)) return;
+    for (int s = threadIdx.x; s < t.n_scenes; s += blockDim.x) *t.scenes[s].acc[1 - cur].count = 0;
+    if (*(volatile uint32_t*)words == 0u) return;
+    for (int s = 0; s < t.n_scenes; ++s) {
+        const SceneDev& M = t.scenes[s];
+        if (*(volatile unsigned long long*)(M.escaped + 2) == 0ull) continue;
+        const GridAcc a = M.acc[cur];
+        const int64_t n = (int64_t)(*a.count) * 64;
+        for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+            const int64_t id = M.g.node_of_block(a.list[e >> 6], (int)(e & 63));
+            a.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+            a.f[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
 }
 
 // ---- exact repair of the light-node rule -----------------------------------------
 //
 // A scene marked by k_grid_update redoes this step's grid from its particles:
-// acc[cur] is zeroed on its listed blocks (the list and the block flags
-// stay), the standalone P2G (momentum and force apart, stress from the SVD
-// of F as in the reference) refills it, and update_grid runs unfolded. The
-// result is the reference's grid for that step, N2 nodes included. Each
-// kernel returns at once when repair[0] is 0, the case of every step whose
-// scenes saw no suspect. The clear kernel also resets the counts of
-// acc[1-cur] that k_grid_update has just zeroed.
-
-__global__ void __launch_bounds__(kGridThreads) k_repair_clear(SceneTable t, int cur, const uint32_t* repair) {
-    const SceneDev& S = t.scenes[blockIdx.y];
-    if (blockIdx.x == 0 && threadIdx.x == 0) *S.acc[1 - cur].count = 0;
-    if (*repair == 0u || S.escaped[2] == 0ull) return;
-    const GridDesc g = S.g;
-    const GridAcc c = S.acc[cur];
-    const int64_t total = (int64_t)(*c.count) * 64;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t id = g.node_of_block(c.list[e >> 6], (int)(e & 63));
-        c.mv[id] = make_float4(0.f, 0.f, 0.f, 0.f);
-        c.f[id] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-}
+// acc[cur] is zeroed on its listed blocks (by the grid update's last CTA; the
+// list and the block flags stay), the standalone P2G (momentum and force
+// apart, stress from the SVD of F as in the reference) refills it, and
+// update_grid runs unfolded. The result is the reference's grid for that
+// step, N2 nodes included. Each kernel returns at once when words[0] is 0,
+// the case of every step whose scenes saw no suspect.
 
 // Standalone P2G of the marked scenes, CTAs striding over the table's
 // 128-particle units (stencil writes outside the box were already counted by
 // the fused kernel, so they are not counted again).
-__global__ void __launch_bounds__(kParticleCTA) k_repair_p2g(SceneTable t, int cur, int sel, const uint32_t* repair) {
-    if (*repair == 0u) return;
+__global__ void __launch_bounds__(kParticleCTA) k_repair_p2g(SceneTable t, int cur, int sel, const uint32_t* words) {
+    if (*words == 0u) return;
     const int64_t units = t.cta_prefix[t.n_scenes];
     for (int64_t unit = blockIdx.x; unit < units; unit += gridDim.x) {
         const int s = scene_of_cta(t, unit);
@@ -289,8 +292,8 @@ __global__ void __launch_bounds__(kParticleCTA) k_repair_p2g(SceneTable t, int c
 
 // Unfolded update_grid of the marked scenes; the last CTA to finish clears
 // the marks for the next step.
-__global__ void __launch_bounds__(kGridThreads) k_repair_update(SceneTable t, int cur, uint32_t* repair) {
-    if (*repair == 0u) return;
+__global__ void __launch_bounds__(kGridThreads) k_repair_update(SceneTable t, int cur, uint32_t* words) {
+    if (*words == 0u) return;
     const SceneDev& S = t.scenes[blockIdx.y];
     if (S.escaped[2] != 0ull) {
         const GridAcc c = S.acc[cur];
@@ -299,25 +302,10 @@ __global__ void __launch_bounds__(kGridThreads) k_repair_update(SceneTable t, in
              e += (int64_t)gridDim.x * blockDim.x)
             update_node(S.g, c, S.mat, S.dt, false, c.list[e >> 6], (int)(e & 63));
     }
-    __shared__ bool last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(repair + 1, 1u) == gridDim.x * gridDim.y - 1;
-    }
-    __syncthreads();
-    if (!last) return;
+    if (!last_cta(words + 2)) return;
     for (int s = threadIdx.x; s < t.n_scenes; s += blockDim.x) t.scenes[s].escaped[2] = 0ull;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        repair[1] = 0u;
-        repair[0] = 0u;
-    }
-}
-
-__global__ void k_reset_counts(SceneTable t, int parity) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < t.n_scenes) *t.scenes[s].acc[parity].count = 0;
+    if (threadIdx.x == 0) words[0] = 0u;
 }
 
 // ---- standalone G2P ---------------------------------------------------------------
@@ -1001,12 +989,8 @@ void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool f
     const int64_t cap = std::max<int64_t>(4, 148 * 8 / t.n_scenes);
     const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, cap));
     const dim3 grid(gx, (unsigned)t.n_scenes);
-    k_grid_update<<<grid, kGridThreads, 0, st>>>(t, cur, folded, folded && repair ? repair->word : nullptr);
-    if (!folded || !repair) {
-        k_reset_counts<<<nblk(t.n_scenes, 128), 128, 0, st>>>(t, 1 - cur);
-        return;
-    }
-    k_repair_clear<<<grid, kGridThreads, 0, st>>>(t, cur, repair->word);
+    k_grid_update<<<grid, kGridThreads, 0, st>>>(t, cur, folded, repair->word);
+    if (!folded) return;
     if (repair->n_ctas > 0) {
         const int64_t ctas = std::min<int64_t>(repair->n_ctas, (int64_t)repair->num_sms * 8);
         k_repair_p2g<<<(unsigned)ctas, kParticleCTA, 0, st>>>(t, cur, repair->sel, repair->word);

@@ -490,10 +490,23 @@ __global__ void __launch_bounds__(64) k_m1(SceneTable t, const M1Params* params,
     m1_candidate_block(t, params[body], cb, cur, acc_all + 7 * body);
 }
 
-// One body, its parameters passed by value (no upload before the launch).
+// One body, its parameters passed by value (no upload before the launch);
+// the last CTA turns the sums into the reaction and zeroes them.
 __global__ void __launch_bounds__(64) k_m1_one(SceneTable t, const __grid_constant__ M1Params P, int cur,
-                                               double* acc) {
+                                               double* acc, bm_reaction_t* out, uint32_t* counter) {
     m1_candidate_block(t, P, blockIdx.x, cur, acc);
+    if (!last_cta(counter)) return;
+    if (threadIdx.x == 0) {
+        volatile double* a = acc;
+        bm_reaction_t r;
+        for (int q = 0; q < 3; ++q) {
+            r.force[q] = (float)a[q];
+            r.torque[q] = (float)a[3 + q];
+        }
+        r.nodes_inside = (int32_t)a[6];
+        *out = r;
+        for (int q = 0; q < 7; ++q) a[q] = 0.0;
+    }
 }
 
 // The reactions from the FP64 sums, which are zeroed after reading so that
@@ -648,10 +661,12 @@ void launch_m1(const SceneTable& t, const M1Params* d_params, int n_bodies, int6
                                                                              n_bodies);
 }
 
-void launch_m1_one(const SceneTable& t, const M1Params& P, int cur, double* d_acc, cudaStream_t st) {
+bool launch_m1_one(const SceneTable& t, const M1Params& P, int cur, double* d_acc, bm_reaction_t* d_out,
+                   uint32_t* counter, cudaStream_t st) {
     const int64_t cand = (int64_t)P.nbi * P.nbj * P.nbk;
-    if (!P.active || cand <= 0) return;
-    k_m1_one<<<(unsigned)cand, 64, 0, st>>>(t, P, cur, d_acc);
+    if (!P.active || cand <= 0) return false;
+    k_m1_one<<<(unsigned)cand, 64, 0, st>>>(t, P, cur, d_acc, d_out, counter);
+    return true;
 }
 
 void launch_m1_flat(const SceneTable& t, const M1Params* d_params, int n_bodies, const int64_t* d_cand_prefix,

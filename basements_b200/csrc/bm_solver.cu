@@ -101,7 +101,15 @@ bm_status_t do_m1(bm_solver* s, int n_bodies, const bm_collider_t* bodies, float
     }
     // (the FP64 sums in d_acc are zero: the last finalize zeroed them)
     if (any_active && n_bodies == 1) {
-        s->w.timed("m1_coupler", [&] { launch_m1_one(s->w.table(), hp[0], s->w.cur, s->d_acc, s->w.stream); });
+        // one launch: the M1 kernel's last CTA writes the reaction
+        bool launched = false;
+        s->w.timed("m1_coupler", [&] {
+            launched = launch_m1_one(s->w.table(), hp[0], s->w.cur, s->d_acc, s->d_react, s->w.d_repair + 3,
+                                     s->w.stream);
+        });
+        if (!launched) launch_reaction_finalize(s->d_acc, n_bodies, s->d_react, s->w.stream);
+        s->view = s->w.cur;
+        return launch_status("m1");
     } else if (any_active) {
         BM_CHECK_CUDA(cudaMemcpyAsync(s->d_params, hp.data(), sizeof(M1Params) * n_bodies, cudaMemcpyHostToDevice,
                                       s->w.stream));

@@ -190,8 +190,8 @@ bm_status_t World::init() {
     BM_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     BM_CHECK_CUDA(cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking));
     BM_CHECK_CUDA(cudaEventCreateWithFlags(&upload_done, cudaEventDisableTiming));
-    BM_CHECK_CUDA(cudaMalloc((void**)&d_repair, 2 * sizeof(uint32_t)));
-    BM_CHECK_CUDA(cudaMemsetAsync(d_repair, 0, 2 * sizeof(uint32_t), stream));
+    BM_CHECK_CUDA(cudaMalloc((void**)&d_repair, kWorldWords * sizeof(uint32_t)));
+    BM_CHECK_CUDA(cudaMemsetAsync(d_repair, 0, kWorldWords * sizeof(uint32_t), stream));
     return BM_OK;
 }
 

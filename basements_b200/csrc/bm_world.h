@@ -79,8 +79,9 @@ public:
     // particle rows back into pageable host arrays and upload_bytes sends
     // them up.
     cudaEvent_t read_done[2] = {nullptr, nullptr};
-    // Device words of the light-node repair (LightRepair::word), zero between
-    // steps.
+    // Device words of the grid update, the light-node repair and the
+    // single-body M1 launch (kWorldWords, LightRepair::word), zero between
+    // launches.
     uint32_t* d_repair = nullptr;
     std::vector<SceneHost> scenes;
     int cur = 0;  // accumulation buffer of the current step
