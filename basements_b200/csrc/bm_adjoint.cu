@@ -615,6 +615,10 @@ bm_status_t backward(bm_tape* t, const bm_particles_view_t* dfinal, float* dL_dw
             if (t->has_body) {
                 const bm_collider_t b = body_at(t, n);
                 if ((st = do_m1(s, 1, &b, t->dt)) != BM_OK) break;
+                // the adjoint kernels read this step's M1 parameters on the
+                // device (the one-body coupler passes them by value)
+                BM_CHECK_CUDA(cudaMemcpyAsync(s->d_params, s->h_params.data(), sizeof(M1Params),
+                                              cudaMemcpyHostToDevice, stream));
             }
             BM_CHECK_CUDA(cudaMemsetAsync(adj_gv, 0, sizeof(float4) * t->nodes, stream));
             const Material& mat = s->sc().dev.mat;
