@@ -420,22 +420,17 @@ __device__ __forceinline__ void gather_inside(const float4* __restrict__ src, in
         }
 }
 
-// mark_stencil_blocks for particles in base-node order, per warp. A full warp
-// (warp_mask all ones) takes the box of its lanes' block ranges (redux
-// min/max per axis); when that box, each extent rounded up to a power of two,
-// holds at most 32 blocks, each lane takes one block of it (its lane index
-// split into the three coordinates by shifts) and marks it if some lane's
-// range covers it: a per-axis
-// ballot gives the lanes covering each block coordinate, and a block is
-// covered by the lanes in all three. Otherwise (a partial warp, a wide box,
-// a lane far outside) a lane whose block range equals that of the lane
-// before it leaves the marks to that lane. The allocated flags are skipped
-// for blocks whose covering lanes all have alloc_done (the blocks of a
-// stencil the particle gathered from in full were allocated by its own
-// scatter, or the lane that covered it, one step earlier).
+// mark_stencil_blocks for particles in base-node order: a lane whose block
+// range equals that of the lane before it leaves the marks to that lane, and
+// the allocated flags are skipped when alloc_done (the blocks of a stencil the
+// particle gathered from in full were allocated by its own scatter, or the
+// lane that covered it, one step earlier). (A per-warp form, one block per
+// lane of the warp's block box found by redux min/max and per-axis ballots,
+// measured 8 us slower on the 2M wheel rut: the covered lanes of this form
+// return at once.)
 __device__ __forceinline__ void mark_stencil_blocks_warp(const GridDesc& g, const GridAcc& a, uint8_t* alloc,
                                                          const int base[3], const float wx[3], const float wy[3],
-                                                         const float wz[3], bool alloc_done, unsigned warp_mask) {
+                                                         const float wz[3], bool alloc_done) {
     const int lo0 = base[0] + (wx[0] == 0.0f), hi0 = base[0] + 2 - (wx[2] == 0.0f);
     const int lo1 = base[1] + (wy[0] == 0.0f), hi1 = base[1] + 2 - (wy[2] == 0.0f);
     const int lo2 = base[2] + (wz[0] == 0.0f), hi2 = base[2] + 2 - (wz[2] == 0.0f);
@@ -443,45 +438,10 @@ __device__ __forceinline__ void mark_stencil_blocks_warp(const GridDesc& g, cons
     const int e0 = ((hi0 - g.ox) >> 2) - b0, e1 = ((hi1 - g.oy) >> 2) - b1, e2 = ((hi2 - g.oz) >> 2) - b2;
     const int lane = (int)(threadIdx.x & 31);
     // a 3-node stencil covers one or two blocks per axis (e in {0, 1}); block
-    // indices far outside the box come from a non-finite position
+    // indices far outside the box (a non-finite position) get a key of their
+    // own so that they never stand in for another lane
     const bool near_box = (unsigned)(b0 + 1) <= (unsigned)(g.nbx + 1) && (unsigned)(b1 + 1) <= (unsigned)(g.nby + 1) &&
                           (unsigned)(b2 + 1) <= (unsigned)(g.nbz + 1);
-    if (warp_mask == 0xffffffffu && __all_sync(warp_mask, near_box)) {
-        const int m0 = __reduce_min_sync(warp_mask, b0), m1 = __reduce_min_sync(warp_mask, b1),
-                  m2 = __reduce_min_sync(warp_mask, b2);
-        const int x0 = __reduce_max_sync(warp_mask, b0 + e0) - m0 + 1,
-                  x1 = __reduce_max_sync(warp_mask, b1 + e1) - m1 + 1,
-                  x2 = __reduce_max_sync(warp_mask, b2 + e2) - m2 + 1;
-        // log2 of each extent rounded up to a power of two
-        const int l0 = x0 > 1 ? 32 - __clz(x0 - 1) : 0, l1 = x1 > 1 ? 32 - __clz(x1 - 1) : 0,
-                  l2 = x2 > 1 ? 32 - __clz(x2 - 1) : 0;
-        if (l0 + l1 + l2 <= 5) {
-            const int c2 = lane & ((1 << l2) - 1), c1 = (lane >> l2) & ((1 << l1) - 1), c0 = lane >> (l1 + l2);
-            unsigned cov0 = 0u, cov1 = 0u, cov2 = 0u;
-            for (int v = 0; v < x0; ++v) {
-                const unsigned bal = __ballot_sync(warp_mask, b0 <= m0 + v && m0 + v <= b0 + e0);
-                if (v == c0) cov0 = bal;
-            }
-            for (int v = 0; v < x1; ++v) {
-                const unsigned bal = __ballot_sync(warp_mask, b1 <= m1 + v && m1 + v <= b1 + e1);
-                if (v == c1) cov1 = bal;
-            }
-            for (int v = 0; v < x2; ++v) {
-                const unsigned bal = __ballot_sync(warp_mask, b2 <= m2 + v && m2 + v <= b2 + e2);
-                if (v == c2) cov2 = bal;
-            }
-            const unsigned need_alloc = __ballot_sync(warp_mask, !alloc_done);
-            const unsigned cov = cov0 & cov1 & cov2;
-            const int i = m0 + c0, j = m1 + c1, k = m2 + c2;
-            if (c0 < x0 && c1 < x1 && c2 < x2 && cov != 0u && (unsigned)i < (unsigned)g.nbx && (unsigned)j < (unsigned)g.nby &&
-                (unsigned)k < (unsigned)g.nbz) {
-                const int64_t blk = g.block_of(i, j, k);
-                if ((cov & need_alloc) != 0u && alloc[blk] == 0) alloc[blk] = 1;
-                touch_block(a, blk);
-            }
-            return;
-        }
-    }
     const unsigned long long key = near_box ? ((unsigned long long)(b0 & 0xFFFFF) << 43) |
                                                   ((unsigned long long)(b1 & 0xFFFFF) << 23) |
                                                   ((unsigned long long)(b2 & 0xFFFFF) << 3) |
@@ -521,9 +481,6 @@ __device__ __forceinline__ void mark_stencil_blocks_warp(const GridDesc& g, cons
 // separately).
 template <bool Fast>
 __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
-    // the lanes of this warp that hold a particle (the others returned before
-    // the call); every one of them reaches the block marking at the end
-    const unsigned warp_mask = __activemask();
     const GridDesc& g = S.g;
     const FusedScene& ps = S;
     int dropped = 0;
@@ -724,8 +681,7 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
             }
         }
     }
-    __syncwarp(warp_mask);
-    mark_stencil_blocks_warp(g, S.next, S.alloc, base, wgt[0], wgt[1], wgt[2], same_base && gather_full, warp_mask);
+    mark_stencil_blocks_warp(g, S.next, S.alloc, base, wgt[0], wgt[1], wgt[2], same_base && gather_full);
     if (!fin) atomicOr(S.status, ERR_NONFINITE);
     if (dropped) {
         atomicOr(S.status, ERR_ESCAPE);
@@ -991,11 +947,12 @@ void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool f
     const dim3 grid(gx, (unsigned)t.n_scenes);
     k_grid_update<<<grid, kGridThreads, 0, st>>>(t, cur, folded, repair->word);
     if (!folded) return;
+    // (grids sized for a quick return: the repair is rare, the launch is not)
     if (repair->n_ctas > 0) {
-        const int64_t ctas = std::min<int64_t>(repair->n_ctas, (int64_t)repair->num_sms * 8);
+        const int64_t ctas = std::min<int64_t>(repair->n_ctas, (int64_t)repair->num_sms * 2);
         k_repair_p2g<<<(unsigned)ctas, kParticleCTA, 0, st>>>(t, cur, repair->sel, repair->word);
     }
-    k_repair_update<<<grid, kGridThreads, 0, st>>>(t, cur, repair->word);
+    k_repair_update<<<dim3(std::min(gx, 16u), (unsigned)t.n_scenes), kGridThreads, 0, st>>>(t, cur, repair->word);
 }
 
 void launch_g2p(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st) {
