@@ -941,8 +941,12 @@ void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStrea
 void launch_grid_update(const SceneTable& t, int64_t max_blocks, int cur, bool folded, cudaStream_t st,
                         const LightRepair* repair) {
     if (t.n_scenes <= 0) return;
+    // one grid row per scene; a row needs no more CTAs than the largest
+    // scene's listed nodes (both accumulators) fill, and at least 32 CTAs per
+    // scene keep a table of many scenes balanced (a scene with fewer listed
+    // blocks leaves its extra CTAs idle at once)
     const int64_t want = (2 * max_blocks * 64 + kGridThreads - 1) / kGridThreads;
-    const int64_t cap = std::max<int64_t>(4, 148 * 8 / t.n_scenes);
+    const int64_t cap = std::max<int64_t>(32, 148 * 8 / t.n_scenes);
     const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, cap));
     const dim3 grid(gx, (unsigned)t.n_scenes);
     k_grid_update<<<grid, kGridThreads, 0, st>>>(t, cur, folded, repair->word);

@@ -116,7 +116,7 @@ BM_API bm_status_t bm_solver_get_domain(bm_solver_t* s, bm_domain_t* out);
 /* Margin (nodes per side, default 16) used when the box is auto-sized. */
 BM_API bm_status_t bm_solver_set_auto_margin(bm_solver_t* s, int32_t margin_nodes);
 /* Particles are reordered by stencil base node (grid order) every `steps`
- * steps (default 16; 1 = every step, 0 = only when particles are added or
+ * steps (default 32; 1 = every step, 0 = only when particles are added or
  * overwritten), so that neighbouring threads share stencil nodes. The order
  * only changes speed and the order of the FP32 reductions. */
 BM_API bm_status_t bm_solver_set_sort_interval(bm_solver_t* s, int32_t steps);

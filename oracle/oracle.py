@@ -110,6 +110,10 @@ def load(kind: str):
         api["tape_free"] = fn("tape_free", None, C.c_void_p)
         api["solver_use_tape"] = fn("solver_use_tape", None, C.c_void_p, C.c_void_p, C.c_int)
         api["tape_status"] = fn("tape_status", None, C.c_void_p, C.POINTER(C.c_int64))
+        api["tape_export"] = fn("tape_export", None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.POINTER(C.c_int64))
+        api["tape_import"] = fn("tape_import", None, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                C.c_void_p)
     _loaded[kind] = api
     return api
 
@@ -315,6 +319,23 @@ class DecisionTape:
         out = (C.c_int64 * 4)()
         self.api["tape_status"](self.t, out)
         return int(out[0]), int(out[1]), int(out[2]), int(out[3]) & ((1 << 40) - 1), bool(out[3] >> 40)
+
+    def export(self):
+        """(SVD codes uint16, inside keys int64, offsets int64) of the record."""
+        sz = (C.c_int64 * 3)()
+        self.api["tape_export"](self.t, None, None, None, sz)
+        svd = np.empty(sz[0], np.uint16)
+        keys = np.empty(sz[2], np.int64)
+        offs = np.empty(sz[1] + 1, np.int64)
+        self.api["tape_export"](self.t, svd.ctypes.data, keys.ctypes.data, offs.ctypes.data, sz)
+        return svd, keys, offs
+
+    def load(self, svd, keys, offs):
+        """Replace the record with arrays from export() (of either checker)."""
+        svd = np.ascontiguousarray(svd, np.uint16)
+        keys = np.ascontiguousarray(keys, np.int64)
+        offs = np.ascontiguousarray(offs, np.int64)
+        self.api["tape_import"](self.t, len(svd), svd.ctypes.data, len(offs) - 1, keys.ctypes.data, offs.ctypes.data)
 
     def close(self):
         if self.t:

@@ -100,6 +100,13 @@ ORC_EXPORT void* ORC(tape_new)(void);
 ORC_EXPORT void ORC(tape_free)(void* t);
 ORC_EXPORT void ORC(solver_use_tape)(void* h, void* t, int mode);
 ORC_EXPORT void ORC(tape_status)(void* t, int64_t* out4);
+/* Restatement only: a tape's content as arrays (SVD codes; coupler inside sets
+ * flattened, offsets of n_calls + 1; NULL arrays: sizes only, into sizes3 =
+ * {SVD codes, coupler calls, keys}) and back, so that one checker's record can
+ * be replayed by the other. */
+ORC_EXPORT void ORC(tape_export)(void* t, uint16_t* svd, int64_t* keys, int64_t* offsets, int64_t* sizes3);
+ORC_EXPORT void ORC(tape_import)(void* t, int64_t n_svd, const uint16_t* svd, int64_t n_calls, const int64_t* keys,
+                                 const int64_t* offsets);
 /* SVD of n row-major 3x3 matrices: U (n*9), sigma (n*3), V (n*9). */
 ORC_EXPORT void ORC(svd)(int64_t n, const float* F, float* U, float* S, float* V);
 

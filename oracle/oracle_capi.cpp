@@ -11,6 +11,8 @@
 #include "oracle_api.h"
 #include "mpm_oracle.hpp"
 
+#include <cstring>
+
 #ifndef ORACLE_REAL
 #define ORACLE_REAL float
 #endif
@@ -153,6 +155,37 @@ ORC_EXPORT void orc_solver_use_tape(void* h, void* t, int mode) {
     s->log_store.tape = T;
     s->log = &s->log_store;
 }
+// Copies of a tape's content, so that a tape recorded by one checker (the
+// float restatement) can be replayed by another (the double one): the SVD
+// codes, the inside sets flattened with their offsets (inside.size() + 1).
+// Pass NULL arrays to read the sizes first.
+ORC_EXPORT void orc_tape_export(void* t, uint16_t* svd, int64_t* keys, int64_t* offsets, int64_t* sizes3) {
+    const DecisionTape* T = static_cast<const DecisionTape*>(t);
+    int64_t nk = 0;
+    for (const auto& v : T->inside) nk += (int64_t)v.size();
+    sizes3[0] = (int64_t)T->svd.size();
+    sizes3[1] = (int64_t)T->inside.size();
+    sizes3[2] = nk;
+    if (svd) std::memcpy(svd, T->svd.data(), sizeof(uint16_t) * T->svd.size());
+    if (keys && offsets) {
+        int64_t o = 0;
+        for (size_t c = 0; c < T->inside.size(); ++c) {
+            offsets[c] = o;
+            for (int64_t k : T->inside[c]) keys[o++] = k;
+        }
+        offsets[T->inside.size()] = o;
+    }
+}
+ORC_EXPORT void orc_tape_import(void* t, int64_t n_svd, const uint16_t* svd, int64_t n_calls, const int64_t* keys,
+                                const int64_t* offsets) {
+    DecisionTape* T = static_cast<DecisionTape*>(t);
+    T->svd.assign(svd, svd + n_svd);
+    T->inside.assign((size_t)n_calls, {});
+    for (int64_t c = 0; c < n_calls; ++c) T->inside[c].assign(keys + offsets[c], keys + offsets[c + 1]);
+    T->svd_pos = T->inside_pos = 0;
+    T->overrun = false;
+}
+
 ORC_EXPORT void orc_tape_status(void* t, int64_t* out4) {
     const DecisionTape* T = static_cast<const DecisionTape*>(t);
     out4[0] = (int64_t)T->svd.size();

@@ -44,15 +44,15 @@ def _frozen_job(args):
     Returns (dL, step taken, replays consistent)."""
     from oracle import oracle as O
 
-    sc, body, wp, steps, target, k, a, eps = args
+    sc, body, wp, steps, target, k, a, eps, branch = args
     tape = O.DecisionTape("f64")
 
-    def loss(w, mode):
-        c = O.CpuSolver("f64", sc.dx)
+    def loss(w, mode, kind="f64", t=tape):
+        c = O.CpuSolver(kind, sc.dx)
         c.set_material(sc.E, sc.nu, sc.rho)
         c.set_plastic_alpha(sc.alpha)
         c.add_particles(sc.position, None, sc.mass)
-        c.use_tape(tape, mode)
+        c.use_tape(t, mode)
         for n in range(steps):
             b = scenes.body_on_path(body, w, steps, sc.dt, n)
             c.p2g(sc.dt)
@@ -63,7 +63,15 @@ def _frozen_job(args):
         c.close()
         return scenes.heightfield_loss(pos, target)[0]
 
-    loss(wp, "record")
+    if branch == "f32":
+        # the branch of the float restatement's run (the decisions an FP32
+        # forward takes), replayed by the double runs
+        t32 = O.DecisionTape("f32")
+        loss(wp, "record", "f32", t32)
+        tape.load(*t32.export())
+        t32.close()
+    else:
+        loss(wp, "record")
     hi, lo = wp.copy(), wp.copy()
     hi[k, a] = np.float32(float(wp[k, a]) + eps)
     lo[k, a] = np.float32(float(wp[k, a]) - eps)
@@ -78,7 +86,7 @@ def _frozen_job(args):
     return Lh - Ll, float(hi[k, a]) - float(lo[k, a]), consistent
 
 
-def fd_waypoints_frozen(p, sc, body, wp, steps, target, coords, eps=1e-6):
+def fd_waypoints_frozen(p, sc, body, wp, steps, target, coords, eps=1e-6, branch="f64"):
     """Central differences dL/d waypoint[k, a] of the FP64 run with its
     discontinuous decisions frozen: both sides replay the SVD pair-skip and
     sweep-stop decisions and the coupler's inside sets of the unperturbed run
@@ -86,8 +94,11 @@ def fd_waypoints_frozen(p, sc, body, wp, steps, target, coords, eps=1e-6):
     branch of the algorithm, the branch an adjoint differentiates. (Left
     free, a 1e-6 change of one waypoint flips hundreds of SVD decisions of
     the 262k-particle tine pass, each adding its jump / 2 eps.) Returns the
-    differences and whether every replay consumed exactly the record."""
-    res = p.map(_frozen_job, [(sc, body, wp, steps, target, k, a, eps) for k, a in coords])
+    differences and whether every replay consumed exactly the record.
+    branch="f32" takes the decisions from a run of the float restatement
+    instead (both sides still computed in double): the branch an FP32 forward
+    follows."""
+    res = p.map(_frozen_job, [(sc, body, wp, steps, target, k, a, eps, branch) for k, a in coords])
     return np.array([d / st for d, st, _ in res]), all(ok for _, _, ok in res)
 
 
