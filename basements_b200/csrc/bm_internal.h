@@ -273,9 +273,10 @@ static_assert(sizeof(FusedPack) <= 32000, "the pack fits the kernel-parameter li
 // Single scene, its view passed by value; many scenes, host arrays of the
 // views (one per scene) for this (cur, sel) and the table's CTA prefix: one
 // launch per pack of scenes.
-void launch_g2p2g_one(const FusedScene& scene, bool fast_math, int variant, cudaStream_t st);
+// `reverse` runs the CTAs in the opposite order (alternated step by step).
+void launch_g2p2g_one(const FusedScene& scene, bool fast_math, int variant, bool reverse, cudaStream_t st);
 void launch_g2p2g_many(const FusedScene* views, const int64_t* prefix, int n_scenes, bool fast_math, int variant,
-                       cudaStream_t st);
+                       bool reverse, cudaStream_t st);
 // Counting sort of every scene's particles by stencil base node, from
 // store[sel] into store[1-sel].
 void launch_sort(const SceneTable& t, int64_t n_ctas, int sel, const SortBuffers& sb, cudaStream_t st);

@@ -654,10 +654,10 @@ bm_status_t World::g2p2g(bool fast_math, int variant) {
         if (scenes.size() == 1) {
             SceneDev d = scenes[0].dev;
             d.mat = material(scenes[0]);
-            launch_g2p2g_one(fused_view(d, cur, sel), fast_math, variant, stream);
+            launch_g2p2g_one(fused_view(d, cur, sel), fast_math, variant, cur == 1, stream);
         } else {
             launch_g2p2g_many(h_views[cur][sel].data(), prefix.data(), (int)scenes.size(), fast_math, variant,
-                              stream);
+                              cur == 1, stream);
         }
     });
     cur = 1 - cur;
