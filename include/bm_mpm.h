@@ -126,9 +126,13 @@ BM_API bm_status_t bm_solver_set_sort_interval(bm_solver_t* s, int32_t steps);
  * accuracy bars against the reference (mode 1 drifts about 2.5x further over
  * 1000 steps) and mode 1 saves under 2% of the step on B200. */
 BM_API bm_status_t bm_solver_set_math_mode(bm_solver_t* s, int32_t mode);
-/* Launch shape of the fused G2P + P2G kernel (threads per CTA x minimum
- * CTAs per SM), one of bm_launch_variant_count(); chosen by the autotuner of
- * the batched form or set here. */
+/* Launch shape of the fused G2P + P2G kernel, one of
+ * bm_launch_variant_count(): threads per CTA x minimum CTAs per SM, and the
+ * order of the particles over a CTA's lanes. The second half of the variants
+ * repeat the shapes of the first half with interleaved lanes (a warp takes
+ * every other particle of 64 consecutive ones; named "<shape>/i2"), which
+ * pays at high particle counts per cell. Chosen by the autotuner of the
+ * batched form or set here; the plain solver's default is 128x7. */
 BM_API bm_status_t bm_solver_set_launch_variant(bm_solver_t* s, int32_t variant);
 BM_API int32_t bm_launch_variant_count(void);
 BM_API const char* bm_launch_variant_name(int32_t variant);
@@ -373,7 +377,8 @@ typedef struct bm_server_config {
     double hbm_budget_bytes;  /* admission budget, default 150e9 */
     int32_t max_active;       /* most co-resident scenes, default 1024 */
     int32_t sort_interval;    /* steps between regroupings, default 16 */
-    int32_t variant;          /* launch shape of the fused kernel, default 1 */
+    int32_t variant;          /* launch variant of the fused kernel (bm_solver_set_launch_variant),
+                                 default 128x7/i2; negative: the default */
 } bm_server_config_t;
 
 typedef enum bm_request_state {

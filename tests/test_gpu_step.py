@@ -322,6 +322,27 @@ def test_bin_regrouping_interval_does_not_change_results():
         assert s.sync() == (0, 0)
 
 
+def test_every_launch_variant_matches_the_reference():
+    """Every launch shape of the fused kernel, in both lane orders (the second
+    half of the variants interleave pairs of warps), gives the reference's
+    particles; the particle count leaves the last CTA partly empty."""
+    names = bm.launch_variants()
+    half = len(names) // 2
+    assert half * 2 == len(names)
+    assert all(n == names[i] + "/i2" for i, n in enumerate(names[half:]))
+    sc = scenes.sand_column()
+    keep = sc.n - 37
+    ref = cpu_solver(REF, sc.dx, sc.position[:keep], None, sc.mass[:keep], sc.E, sc.nu, sc.rho, sc.alpha)
+    ref.step(sc.dt, 40)
+    pr = ref.get_particles()["position"]
+    for v, name in enumerate(names):
+        s = gpu_solver(sc.dx, sc.position[:keep], None, sc.mass[:keep], sc.E, sc.nu, sc.rho, sc.alpha)
+        s.set_launch_variant(v)
+        s.step(sc.dt, 40)
+        assert max_err_dx(s.get_particles()["position"], pr, sc.dx) < POS_TOL_100, name
+        assert s.sync() == (0, 0), name
+
+
 def test_particles_leaving_their_tile_take_the_global_path():
     """Fast particles never regrouped drift many cells away from their bin's
     shared-memory tile; the global-memory path must give the reference result."""
