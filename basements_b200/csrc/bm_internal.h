@@ -75,9 +75,20 @@ struct GridDesc {
             return -1;
         return node_rel(ri, rj, rk);
     }
+    // Block coordinates of block b (unsigned 32-bit division: a box holds
+    // fewer than 2^31 nodes, so fewer than 2^25 blocks; 64-bit division would
+    // cost several times the instructions in the per-node kernels).
+    __host__ __device__ __forceinline__ void block_coords(int64_t b, int& bi, int& bj, int& bk) const {
+        const unsigned ub = (unsigned)b, nz = (unsigned)nbz, ny = (unsigned)nby;
+        const unsigned q = ub / nz, r = q / ny;
+        bk = (int)(ub - q * nz);
+        bj = (int)(q - r * ny);
+        bi = (int)r;
+    }
     // Node of block b at local slot t = li*16 + lj*4 + lk.
     __host__ __device__ __forceinline__ int64_t node_of_block(int64_t b, int t) const {
-        const int bk = (int)(b % nbz), bj = (int)((b / nbz) % nby), bi = (int)(b / ((int64_t)nbz * nby));
+        int bi, bj, bk;
+        block_coords(b, bi, bj, bk);
         return node_rel(4 * bi + (t >> 4), 4 * bj + ((t >> 2) & 3), 4 * bk + (t & 3));
     }
     // Block of a linear node index.

@@ -188,7 +188,7 @@ __device__ __forceinline__ void update_node(const GridDesc& g, const GridAcc& c,
     v1 = v1 + mat.gy * dt;
     v2 = v2 + mat.gz * dt;
     const int lj = (tt >> 2) & 3;
-    const int bj = (int)((b / g.nbz) % g.nby);
+    const int bj = (int)(((unsigned)b / (unsigned)g.nbz) % (unsigned)g.nby);
     const int j = g.oy + 4 * bj + lj;
     const float node_y = ((float)j + 0.5f) * g.dx;
     if (node_y < g.dx && v1 < 0.0f) {
