@@ -534,7 +534,7 @@ BM_API bm_status_t bm_batch_autotune(bm_batch_t* b, int32_t trial_steps, bm_tune
     }
     const int nv = fused_variant_count();
     const int32_t intervals[] = {8, 16, 32};
-    const int nshapes = nv / 2;  // the shapes, then the same shapes with interleaved lanes
+
     const int32_t shifts[] = {0, 1};
     int32_t best_v = b->variant, best_k = b->sort_interval, best_s = b->w.scenes[0].dev.bin_shift;
     float best_ms = 1e30f;
@@ -553,24 +553,14 @@ BM_API bm_status_t bm_batch_autotune(bm_batch_t* b, int32_t trial_steps, bm_tune
         if (r == BM_OK) *ms /= (float)T;
         return r;
     };
-    // launch shape first, then its interleaved-lane twin, then bin size and
-    // interval with the best of those
-    for (int v = 0; v < nshapes && st == BM_OK; ++v) {
+    // launch variant first (every shape in both lane orders), then bin size
+    // and interval with the best of those
+    for (int v = 0; v < nv && st == BM_OK; ++v) {
         float ms = 0;
         st = trial(v, 16, best_s, &ms);
         if (st == BM_OK && ms < best_ms) {
             best_ms = ms;
             best_v = v;
-            best_k = 16;
-        }
-    }
-    if (st == BM_OK) {
-        const int vi = fused_variant_interleaved(best_v);
-        float ms = 0;
-        st = trial(vi, 16, best_s, &ms);
-        if (st == BM_OK && ms < best_ms) {
-            best_ms = ms;
-            best_v = vi;
             best_k = 16;
         }
     }

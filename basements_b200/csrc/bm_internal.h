@@ -258,8 +258,6 @@ int fused_variant_count();
 const char* fused_variant_name(int v);
 // Index of the launch variant with this shape and lane order (0 if none).
 int fused_variant_index(int threads, int min_blocks, int interleave);
-// The variant with v's shape and interleaved lanes.
-int fused_variant_interleaved(int v);
 // The fused kernel's view of one scene with the buffer choice (cur, sel)
 // resolved: exactly the fields it touches, no runtime-indexed arrays.
 struct FusedScene {

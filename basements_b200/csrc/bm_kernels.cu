@@ -970,10 +970,6 @@ int fused_variant_index(int threads, int min_blocks, int interleave) {
             return v;
     return 0;
 }
-int fused_variant_interleaved(int v) {
-    if (v < 0 || v >= kNumFused) return v;
-    return fused_variant_index(kFused[v].threads, kFused[v].min_blocks, 1);
-}
 const char* fused_variant_name(int v) { return (v >= 0 && v < kNumFused) ? kFused[v].name : "?"; }
 
 void launch_p2g(const SceneTable& t, int64_t n_ctas, int cur, int sel, cudaStream_t st, bool only_fresh) {
