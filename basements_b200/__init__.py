@@ -633,7 +633,7 @@ class Batch:
 class Server:
     """Continuous-batching server (bm_server_*)."""
 
-    def __init__(self, hbm_budget_bytes=150e9, max_active=1024, sort_interval=16, variant=-1):
+    def __init__(self, hbm_budget_bytes=150e9, max_active=1024, sort_interval=32, variant=-1):
         cfg = ServerConfig(float(hbm_budget_bytes), int(max_active), int(sort_interval), int(variant))
         self._h = C.c_void_p()
         check(lib().bm_server_create(C.byref(cfg), C.byref(self._h)), "bm_server_create")

@@ -544,7 +544,7 @@ BM_API bm_status_t bm_server_create(const bm_server_config_t* config, bm_server_
     bm_server* s = new bm_server();
     s->cfg.hbm_budget_bytes = 150e9;
     s->cfg.max_active = 1024;
-    s->cfg.sort_interval = 16;
+    s->cfg.sort_interval = 32;  // measured 3 % faster than 16 on the served request mix
     s->cfg.variant = fused_variant_index(128, 7, 1);  // as the batched form's default
     if (config) {
         if (config->hbm_budget_bytes > 0) s->cfg.hbm_budget_bytes = config->hbm_budget_bytes;

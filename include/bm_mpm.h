@@ -376,7 +376,7 @@ typedef struct bm_server bm_server_t;
 typedef struct bm_server_config {
     double hbm_budget_bytes;  /* admission budget, default 150e9 */
     int32_t max_active;       /* most co-resident scenes, default 1024 */
-    int32_t sort_interval;    /* steps between regroupings, default 16 */
+    int32_t sort_interval;    /* steps between regroupings, default 32 */
     int32_t variant;          /* launch variant of the fused kernel (bm_solver_set_launch_variant),
                                  default 128x7/i2; negative: the default */
 } bm_server_config_t;
