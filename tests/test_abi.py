@@ -52,3 +52,15 @@ def test_argument_validation_without_compute():
     assert L.bm_solver_step(None, 0.1) == 1
     assert L.bm_solver_destroy(None) == 1
     assert b"dx" in L.bm_last_error() or b"NULL" in L.bm_last_error()
+
+
+def test_launch_variant_table_pairs_each_shape_with_its_interleaved_twin():
+    """The fused kernel's launch variants (host-side table, no device call):
+    the shapes, then the same shapes with interleaved lanes ("/i2"); the
+    plain solver's default 128x7 is among the first half."""
+    names = bm.launch_variants()
+    half = len(names) // 2
+    assert len(names) == 2 * half and half > 0
+    assert all(re.fullmatch(r"\d+x\d+", n) for n in names[:half])
+    assert names[half:] == [n + "/i2" for n in names[:half]]
+    assert "128x7" in names[:half]
