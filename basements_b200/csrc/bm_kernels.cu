@@ -648,14 +648,34 @@ __device__ __forceinline__ void g2p2g_particle(const FusedScene& S, int64_t p) {
             // fringe of the material get here. The gathered masses come from
             // the gather's bits: no load, so the loop waits on nothing.
             if (!all_heavy) {
+                // the nodes that take a record, as bits in stencil order (bit
+                // 26 - n for node n): a light contribution (same product as
+                // the scatter's mass lane) at a node that was not heavy; the
+                // loop then visits only those (a fringe particle has a few of
+                // its 27), where visiting all 27 held a fringe warp 3x longer
                 const uint32_t not_heavy = same_base ? light : 0x7FFFFFFu;
+                uint32_t rec = 0u;
 #pragma unroll 1
-                for (int n = 0; n < 27; ++n) {
+                for (int i = 0; i < 3; ++i) {
+                    const float wi = pick3(wgt[0], i);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const float wij = wi * wgt[1][j];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const float w = wij * wgt[2][k];
+                            rec = (rec << 1) | (w != 0.0f && w * m <= 1e-6f ? 1u : 0u);
+                        }
+                    }
+                }
+                rec &= not_heavy;
+                while (rec) {
+                    const int bit = 31 - __clz(rec);
+                    rec &= ~(1u << bit);
+                    const int n = 26 - bit;
                     const int i = n / 9, j = (n / 3) % 3, k = n % 3;
                     const float w = pick3(wgt[0], i) * pick3(wgt[1], j) * pick3(wgt[2], k);
-                    if (w == 0.0f || !(w * m <= 1e-6f)) continue;
                     const int64_t off = i * EYZ + j * EZ + k;
-                    if (!((not_heavy >> (26 - n)) & 1u)) continue;
                     const float d0 = pick3(dd[0], i), d1 = pick3(dd[1], j), d2 = pick3(dd[2], k);
                     float S_[9];
 #pragma unroll
