@@ -553,23 +553,38 @@ BM_API bm_status_t bm_batch_autotune(bm_batch_t* b, int32_t trial_steps, bm_tune
         if (r == BM_OK) *ms /= (float)T;
         return r;
     };
-    // launch variant first (every shape in both lane orders), then bin size
-    // and interval with the best of those
+    // launch variant first (every shape in both lane orders) at interval 16,
+    // then the three fastest once more, each keeping the lower of its two
+    // times (one trial's noise, about 1 %, is as large as their differences),
+    // then bin size and interval with the best of those, each timed twice
+    std::vector<std::pair<float, int>> vt;
     for (int v = 0; v < nv && st == BM_OK; ++v) {
         float ms = 0;
         st = trial(v, 16, best_s, &ms);
-        if (st == BM_OK && ms < best_ms) {
-            best_ms = ms;
-            best_v = v;
+        if (st == BM_OK) vt.emplace_back(ms, v);
+    }
+    std::sort(vt.begin(), vt.end());
+    for (size_t q = 0; q < vt.size() && q < 3 && st == BM_OK; ++q) {
+        float ms = 0;
+        st = trial(vt[q].second, 16, best_s, &ms);
+        if (st == BM_OK) vt[q].first = std::min(vt[q].first, ms);
+    }
+    for (size_t q = 0; q < vt.size() && q < 3; ++q)
+        if (vt[q].first < best_ms) {
+            best_ms = vt[q].first;
+            best_v = vt[q].second;
             best_k = 16;
         }
-    }
     for (int32_t sh : shifts)
         for (int32_t k : intervals) {
+            float ms = 1e30f;
+            for (int rep = 0; rep < 2 && st == BM_OK; ++rep) {
+                float t = 0;
+                st = trial(best_v, k, sh, &t);
+                if (st == BM_OK) ms = std::min(ms, t);
+            }
             if (st != BM_OK) break;
-            float ms = 0;
-            st = trial(best_v, k, sh, &ms);
-            if (st == BM_OK && ms < best_ms) {
+            if (ms < best_ms) {
                 best_ms = ms;
                 best_k = k;
                 best_s = sh;
